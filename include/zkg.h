@@ -1,0 +1,185 @@
+/* zkg.h — C ABI of the B200 (sm_100a) BN254 MSM and Fr NTT library.
+ *
+ * The entry points are exactly what a Rust (or any FFI) binding of zk-gpu's public API needs
+ * (src/lib.rs:1-6 re-exports gpu, msm, ntt, group, host). Each declaration names the reference
+ * interface it replaces as path:line within zerotruss/zk-gpu.
+ *
+ * Conventions
+ *  - Plain pointers and sizes; opaque handles; no C++ or torch types.
+ *  - Every fallible call returns ZKG_OK (0) or an error code; zkg_last_error() then returns a
+ *    message for the calling thread. Argument errors carry the same text as the reference's
+ *    panics (tests/invalid_inputs.rs:9-50), so a binding can panic with it unchanged.
+ *  - Memory format (unchanged from the reference): 8 little-endian u32 words per field
+ *    element; affine points are x then y, Fq2 coordinates a then b (x = a + b*u, u^2 = -1);
+ *    the point at infinity is all-zero words (src/msm.rs:182-183, src/group.rs:59-69).
+ *  - Work is queued on the context's single ordered stream and runs asynchronously until a
+ *    read or zkg_ctx_sync, like the reference's wgpu queue (src/gpu.rs:151-155).
+ *  - Results of the MSM are XYZZ points in Montgomery form with R = 2^256 (the reference's
+ *    XYZZ words use R = 2^260; only the affine reading through zkg_xyzz_to_affine* is part of
+ *    the contract, README.md:83-96).
+ */
+#ifndef ZKG_H
+#define ZKG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct zkg_ctx zkg_ctx; /* gpu::Gpu                           src/gpu.rs:6-12   */
+typedef struct zkg_buf zkg_buf; /* wgpu::Buffer of u32 words          src/gpu.rs:57-69  */
+typedef struct zkg_msm zkg_msm; /* msm::Msm plan                      src/msm.rs:25-37  */
+typedef struct zkg_ntt zkg_ntt; /* ntt::Ntt plan                      src/ntt.rs:14-20  */
+
+enum zkg_status {
+  ZKG_OK = 0,
+  ZKG_EINVAL = 1,    /* argument out of range (the reference panics: msm.rs:97-98, ntt.rs:27) */
+  ZKG_ESIZE = 2,     /* buffer too small (msm.rs:273-282, ntt.rs:53-59)                       */
+  ZKG_ECUDA = 3,     /* CUDA runtime failure (wgpu device lost / validation, gpu.rs:44-49)     */
+  ZKG_ENOMEM = 4,    /* device allocation failed                                               */
+  ZKG_ETIMEDOUT = 5, /* a bounded device wait expired                                          */
+  ZKG_ENODEV = 6     /* no usable GPU (Gpu::new_async's "no GPU adapter", gpu.rs:22-30)         */
+};
+
+enum zkg_group {
+  ZKG_G1 = 1, /* group::Group::G1  src/group.rs:11-14 */
+  ZKG_G2 = 2  /* group::Group::G2                     */
+};
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *zkg_last_error(void);
+
+/* ------------------------------------------------------------------ Gpu (src/gpu.rs) */
+
+/* Gpu::new / Gpu::new_async (src/gpu.rs:22-55): context on CUDA device `device`. */
+int zkg_ctx_new(int device, zkg_ctx **out);
+void zkg_ctx_free(zkg_ctx *ctx);
+/* Gpu::wait (src/gpu.rs:151-155): block until every queued call has finished; reports any
+ * device fault that happened since the last check. */
+int zkg_ctx_sync(zkg_ctx *ctx);
+/* Gpu::adapter.name (src/gpu.rs:9): device name, NUL-terminated, truncated to cap. */
+int zkg_ctx_device_name(zkg_ctx *ctx, char *out, size_t cap);
+
+/* Gpu::buffer (src/gpu.rs:57-64): device buffer initialised with `words` u32 words. The host
+ * array may be reused as soon as the call returns. */
+int zkg_buf_new(zkg_ctx *ctx, const uint32_t *data, size_t words, zkg_buf **out);
+/* Gpu::empty_buffer (src/gpu.rs:66-69): zero-filled buffer of `words` words. */
+int zkg_buf_zeroed(zkg_ctx *ctx, size_t words, zkg_buf **out);
+/* wgpu Queue::write_buffer: overwrite words [offset, offset + words) from host memory. */
+int zkg_buf_write(zkg_ctx *ctx, zkg_buf *buf, size_t offset_words, const uint32_t *data, size_t words);
+/* Gpu::read / try_read_async (src/gpu.rs:166-199): blocking copy of the first `words` words. */
+int zkg_buf_read(zkg_ctx *ctx, const zkg_buf *buf, uint32_t *out, size_t words);
+/* wgpu Buffer::size / 4 */
+size_t zkg_buf_words(const zkg_buf *buf);
+/* Device address of the buffer, for interop with other CUDA code on the same device. */
+void *zkg_buf_device_ptr(const zkg_buf *buf);
+/* Frees a buffer made by zkg_buf_new / zkg_buf_zeroed / zkg_msm_upload_bases*. Borrowed
+ * handles (zkg_msm_run's result) are ignored. */
+void zkg_buf_free(zkg_buf *buf);
+
+/* ------------------------------------------------------------------ Msm (src/msm.rs) */
+
+/* Msm::default_window (src/msm.rs:76-80): clamp(log2(max(n,1)) - 5, 11, 16). */
+uint32_t zkg_msm_default_window(size_t n);
+
+/* Msm::upload_bases (src/msm.rs:182-188): affine points in plain coordinates (16 words per G1
+ * point, 32 per G2 point; infinity (0,0)) converted on the device to Montgomery form. */
+int zkg_msm_upload_bases(zkg_ctx *ctx, const uint32_t *plain_xy, size_t words, zkg_buf **out);
+/* Msm::upload_bases_montgomery_256 (src/msm.rs:190-197): coordinates already in Montgomery
+ * form with R = 2^256 (snarkjs / ffjavascript); with this library's R = 2^256 they are used
+ * as they are. */
+int zkg_msm_upload_bases_montgomery_256(zkg_ctx *ctx, const uint32_t *xy, size_t words, zkg_buf **out);
+
+/* Msm::for_group / new / with_item_points (src/msm.rs:82-180). `c` must be in 9..=20;
+ * item_points = 0 picks the work-item size automatically (points accumulated per thread
+ * before partial sums are combined). Fails with the reference's messages: "an MSM needs at
+ * least one point", "window size c must be in 9..=20, got {c}". */
+int zkg_msm_new(zkg_ctx *ctx, int group, size_t n, uint32_t c, uint32_t item_points, zkg_msm **out);
+void zkg_msm_free(zkg_msm *msm);
+/* Msm::group (src/msm.rs:267-269) */
+int zkg_msm_group(const zkg_msm *msm);
+/* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
+ * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,
+ * Montgomery form), overwritten by the next run. Checks sizes first ("scalars buffer holds ...",
+ * "bases buffer holds ..."). */
+int zkg_msm_run(zkg_msm *msm, const zkg_buf *bases, const zkg_buf *scalars, const zkg_buf **result);
+
+typedef struct {
+  char stage[32];
+  double ms;
+} zkg_stage_time;
+/* Msm::profile (src/msm.rs:321-342): runs every stage separately and reports device time per
+ * stage (CUDA events). *count receives the number of stages written (at most cap). */
+int zkg_msm_profile(zkg_msm *msm, const zkg_buf *bases, const zkg_buf *scalars, zkg_stage_time *out, size_t cap,
+                    size_t *count);
+
+/* xyzz_to_affine (src/msm.rs:345-354): 32 result words -> plain affine x, y as 4 LE u64 each.
+ * Returns 1 for a finite point, 0 for infinity (x, y set to zero), negative on error. */
+int zkg_xyzz_to_affine(const uint32_t *words, uint64_t *x, uint64_t *y);
+/* xyzz_to_affine_g2 (src/msm.rs:356-373): 64 words -> x = (x.a, x.b), y = (y.a, y.b), each
+ * coordinate 4 LE u64 (8 u64 per Fq2 value). Returns 1 finite, 0 infinity. */
+int zkg_xyzz_to_affine_g2(const uint32_t *words, uint64_t *x, uint64_t *y);
+
+/* ------------------------------------------------------------------ Ntt (src/ntt.rs) */
+
+/* Ntt::new (src/ntt.rs:26-40): plan for 2^log_n elements, 10 <= log_n <= 27
+ * ("log_n must be in 10..=27"). */
+int zkg_ntt_new(zkg_ctx *ctx, uint32_t log_n, zkg_ntt **out);
+void zkg_ntt_free(zkg_ntt *ntt);
+/* Ntt::log_n (src/ntt.rs:19) */
+uint32_t zkg_ntt_log_n(const zkg_ntt *ntt);
+/* Ntt::forward (src/ntt.rs:42-45): in place, natural order in and out (plain Fr words).
+ * Fails with "data buffer holds ..." if the buffer is smaller than 2^log_n elements. */
+int zkg_ntt_forward(zkg_ntt *ntt, zkg_buf *data);
+/* Ntt::inverse (src/ntt.rs:47-50): in place, includes the 1/n factor. */
+int zkg_ntt_inverse(zkg_ntt *ntt, zkg_buf *data);
+
+/* ------------------------------------------------------------------ runtime helpers (no reference counterpart:
+ * wgpu hides its queue, launches and staging memory) */
+
+/* The context's cudaStream_t, for callers that time or order work with their own CUDA calls. */
+void *zkg_ctx_stream(zkg_ctx *ctx);
+/* Number of kernels this library has launched in this process (all contexts). */
+uint64_t zkg_launch_count(void);
+/* Page-locked host memory for fast host<->device copies (cudaHostAlloc / cudaFreeHost). */
+int zkg_host_alloc(size_t bytes, void **out);
+void zkg_host_free(void *p);
+
+/* Live stage timing: while enabled, every zkg_msm_run records CUDA events around each stage on
+ * the context stream (no synchronisation); zkg_msm_stage_times waits for them, returns the
+ * summed device time per stage over the runs since the last call, and starts a new sum.
+ * *runs receives the number of runs summed. */
+int zkg_msm_set_timing(zkg_msm *msm, int enable);
+int zkg_msm_stage_times(zkg_msm *msm, zkg_stage_time *out, size_t cap, size_t *count, size_t *runs);
+/* The same for the NTT: one entry per pass ("pass 0", "pass 1", ...), forward and inverse
+ * transforms summed together. */
+int zkg_ntt_set_timing(zkg_ntt *ntt, int enable);
+int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *count, size_t *runs);
+
+/* ------------------------------------------------------------------ testing and set-up helpers */
+
+/* Throughput probe of the integer multiply-add pipe (the reference's examples/field_bench.rs
+ * measures mulmods per second the same way): variant 0 = mad.lo.u32, 1 = mad.hi.u32,
+ * 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq Montgomery
+ * products. *ops_per_second receives multiply-adds (or products) per second on the context's
+ * device; the best of five launches over every SM. */
+int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
+
+/* Point operations for the curve tests (the reference's tests/curve.rs:22-44 kernel): for each
+ * of `count` affine pairs (P, Q) in Montgomery form (32 words G1 / 64 words G2 per pair), writes
+ * three XYZZ points: P + Q (mixed add), 2P (double), (P + Q) + 2P (full add). */
+int zkg_test_point_ops(zkg_ctx *ctx, int group, const uint32_t *pairs, size_t count, uint32_t *out);
+
+/* Fixed-base batch multiplication: out[i] = [k_i] G for the standard generator of `group`
+ * (G1 = (1, 2)), as affine points in plain (mont256 = 0) or Montgomery-2^256 (mont256 = 1)
+ * coordinates. Scalars are 8 words each, any 256-bit value. Used to build proving-key-like
+ * bases on the device (the reference's tests build them with arkworks, tests/g2.rs:136). */
+int zkg_generator_multiples(zkg_ctx *ctx, int group, const zkg_buf *scalars, size_t n, int mont256, zkg_buf *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZKG_H */

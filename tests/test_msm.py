@@ -1,0 +1,283 @@
+"""G1 MSM against the oracle (tests/msm.rs:10-67), the property suite
+(tests/properties.rs:150-431) and the full benchmark sizes through the identity
+MSM([k_i]G, s) = [sum_i s_i k_i]G with bases built on the device."""
+import os
+
+import numpy as np
+import pytest
+
+from common import fr_words, gpu_msm, msm_ref, quick, random_fr, random_points
+from oracle import bn254, cpu
+from zk_gpu import Group, Msm, xyzz_to_affine
+from zk_gpu.msm import affine_words
+from zk_gpu.synthetic import generator_multiples, infinity_mask, scalar_distribution, uniform_scalars
+
+pytestmark = pytest.mark.gpu
+R = bn254.R
+
+
+def check(gpu, bases, scalars, c, what):
+    expected = msm_ref("G1", bases, scalars)
+    for item_points in (1024, 7):
+        got = gpu_msm(gpu, bases, scalars, (c, item_points))
+        assert np.array_equal(got, expected), f"{what} (n = {scalars.size // 8}, c = {c}, item_points = {item_points})"
+
+
+def test_random_inputs(gpu):
+    for n, c in [(1000, 9), (4096, 10), (20000, 12), (100000, 14)]:
+        check(gpu, random_points("G1", n, n), random_fr(n + 1, n), c, "random")
+
+
+def test_edge_cases(gpu):
+    n, c = 3000, 10
+    p = random_points("G1", 1, 1)
+    rand = random_points("G1", 2, n)
+    rand_s = random_fr(3, n)
+    check(gpu, rand, fr_words([0] * n), c, "all-zero scalars")
+    check(gpu, rand, fr_words([1] * n), c, "all-one scalars (one huge bucket)")
+    check(gpu, rand, fr_words([R - 1] * n), c, "scalars = r - 1")
+    same = np.tile(p, n)
+    check(gpu, same, rand_s, c, "same base everywhere (forces doublings)")
+    check(gpu, same, fr_words([5] * n), c, "same base, same scalar")
+    check(gpu, rand, fr_words(i % 7 for i in range(n)), c, "tiny scalars")
+    with_inf = rand.copy()
+    with_inf[16 * 3: 16 * 4] = 0
+    with_inf[16 * 100: 16 * 101] = 0
+    check(gpu, with_inf, rand_s, c, "bases containing infinity")
+    negp = np.array(bn254.affine_words("G1", bn254.affine_neg(bn254._FqOps, (bn254.from_words32(p[:8]),
+                                                                            bn254.from_words32(p[8:])))),
+                    dtype=np.uint32)
+    cancel = np.concatenate([p, negp, rand[:16 * 8]])
+    cs = np.concatenate([rand_s[:8], rand_s[:8], np.zeros(64, dtype=np.uint32)])
+    check(gpu, cancel, cs, c, "cancels to the point at infinity")
+
+
+def test_default_parameters(gpu):
+    n = 1 << 17
+    bases, scalars = random_points("G1", 30, n), random_fr(31, n)
+    assert np.array_equal(gpu_msm(gpu, bases, scalars), msm_ref("G1", bases, scalars))
+
+
+def add_affine(a, b):
+    F = bn254._FqOps
+    pa = None if not a.any() else (bn254.from_words32(a[:8]), bn254.from_words32(a[8:16]))
+    pb = None if not b.any() else (bn254.from_words32(b[:8]), bn254.from_words32(b[8:16]))
+    return np.array(bn254.affine_words("G1", bn254.affine_add(F, pa, pb)), dtype=np.uint32)
+
+
+def scal(s: np.ndarray):
+    return [bn254.from_words32(s[8 * i: 8 * i + 8]) for i in range(s.size // 8)]
+
+
+def test_is_linear_in_the_scalars(gpu):
+    n = 3000
+    bases = random_points("G1", 10, n)
+    s, t = random_fr(11, n), random_fr(12, n)
+    sum_ = fr_words((a + b) % R for a, b in zip(scal(s), scal(t)))
+    expected = add_affine(gpu_msm(gpu, bases, s), gpu_msm(gpu, bases, t))
+    assert np.array_equal(gpu_msm(gpu, bases, sum_), expected), "MSM(s + t) != MSM(s) + MSM(t)"
+
+
+def test_is_linear_in_the_bases(gpu):
+    n = 3000
+    p, q = random_points("G1", 13, n), random_points("G1", 14, n)
+    s = random_fr(15, n)
+    sum_ = np.concatenate([add_affine(p[16 * i: 16 * i + 16], q[16 * i: 16 * i + 16]) for i in range(n)])
+    expected = add_affine(gpu_msm(gpu, p, s), gpu_msm(gpu, q, s))
+    assert np.array_equal(gpu_msm(gpu, sum_, s), expected), "MSM(P + Q) != MSM(P) + MSM(Q)"
+
+
+def test_scales_with_a_constant(gpu):
+    n = 3000
+    bases = random_points("G1", 16, n)
+    s = random_fr(17, n)
+    c = 0xABCDEF0123456789ABCDEF
+    scaled = fr_words(x * c % R for x in scal(s))
+    m = gpu_msm(gpu, bases, s)
+    expected = np.array(bn254.affine_words("G1", bn254.scalar_mul(
+        bn254._FqOps, (bn254.from_words32(m[:8]), bn254.from_words32(m[8:])), c)), dtype=np.uint32)
+    assert np.array_equal(gpu_msm(gpu, bases, scaled), expected), "MSM(c * s) != c * MSM(s)"
+
+
+def test_ignores_the_order_of_the_pairs(gpu):
+    n = 5000
+    bases, s = random_points("G1", 18, n), random_fr(19, n)
+    order = np.random.default_rng(20).permutation(n)
+    b2 = bases.reshape(n, 16)[order].reshape(-1)
+    s2 = s.reshape(n, 8)[order].reshape(-1)
+    assert np.array_equal(gpu_msm(gpu, b2, s2), gpu_msm(gpu, bases, s))
+
+
+def test_tiny_inputs(gpu):
+    for n in [1, 2, 3, 7, 17, 255, 256, 257, 1023, 1025]:
+        bases, s = random_points("G1", 21 + n, n), random_fr(22 + n, n)
+        want = msm_ref("G1", bases, s)
+        for plan in [None, (9, 1024), (9, 1)]:
+            assert np.array_equal(gpu_msm(gpu, bases, s, plan), want), f"n = {n}, plan = {plan}"
+
+
+def test_bases_already_in_montgomery_form(gpu):
+    for n in [1, 5, 300, 2000]:
+        bases = random_points("G1", 40 + n, n)
+        bases[16 * (n // 2): 16 * (n // 2) + 16] = 0
+        s = random_fr(41 + n, n)
+        buf = Msm.upload_bases_montgomery_256(gpu, cpu.fq_to_mont256(bases))
+        msm = Msm(gpu, n, Msm.default_window(n))
+        got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, buf, gpu.buffer(s)), 32)))
+        assert np.array_equal(got, msm_ref("G1", bases, s)), f"n = {n}"
+
+
+def test_huge_buckets(gpu):
+    for n in [17, 300, 5000]:
+        bases = random_points("G1", 50 + n, n)
+        rnd = np.random.default_rng(n)
+        same = fr_words([7] * n)
+        ones = fr_words([1] * n)
+        mostly = fr_words(int(v) if i % 50 == 0 else 3 for i, v in enumerate(rnd.integers(0, 1 << 62, size=n)))
+        for scalars in (same, ones, mostly):
+            want = msm_ref("G1", bases, scalars)
+            for plan in [(9, 1), (10, 3), None]:
+                assert np.array_equal(gpu_msm(gpu, bases, scalars, plan), want), f"n = {n}, plan = {plan}"
+
+
+def test_nearly_empty_top_window(gpu):
+    n = 20000
+    bases, s = random_points("G1", 60, n), random_fr(61, n)
+    want = msm_ref("G1", bases, s)
+    for plan in [(14, 8), (14, 1), (11, 8)]:
+        assert np.array_equal(gpu_msm(gpu, bases, s, plan), want), f"plan = {plan}"
+
+
+def test_generator_multiples_2_18(gpu):
+    """Big enough for many accumulate segments per bucket and several merge levels."""
+    n = 1 << 18
+    k = np.array([w for i in range(1, n + 1) for w in bn254.words32(i)], dtype=np.uint32)
+    bases = cpu.generator_multiples("G1", k)
+    s = random_fr(62, n)
+    want = msm_ref("G1", bases, s)
+    for plan in [None, (15, 8)]:
+        assert np.array_equal(gpu_msm(gpu, bases, s, plan), want), f"plan = {plan}"
+
+
+def boundary_scalars(c):
+    out = [0, 1, R - 1, R - 2, R - (1 << c)]
+    for j in range(1, -(-254 // c) + 1):
+        for k in (c * j - 1, c * j):
+            p = pow(2, k, R)
+            out += [(p - 1) % R, p, (p + 1) % R]
+    return out
+
+
+def test_window_boundaries(gpu):
+    for c in range(9, 17):
+        vals = boundary_scalars(c) * 2
+        s = fr_words(vals)
+        bases = random_points("G1", 70 + c, len(vals))
+        want = msm_ref("G1", bases, s)
+        for item_points in (1024, 3):
+            assert np.array_equal(gpu_msm(gpu, bases, s, (c, item_points)), want), f"c = {c}, items = {item_points}"
+
+
+def test_result_does_not_depend_on_the_window_size(gpu):
+    n = 6000
+    bases, s = random_points("G1", 80, n), random_fr(81, n)
+    want = msm_ref("G1", bases, s)
+    for c in range(9, 21):
+        assert np.array_equal(gpu_msm(gpu, bases, s, (c, 1024)), want), f"window size c = {c}"
+
+
+def test_plan_can_be_reused(gpu):
+    n = 4000
+    bases = random_points("G1", 90, n)
+    base_buf = Msm.upload_bases(gpu, bases)
+    msm = Msm(gpu, n, 11)
+    sets = [random_fr(91, n), fr_words([0] * n), fr_words([1] * n), random_fr(92, n)]
+    for rnd in range(2):
+        for i, s in enumerate(sets):
+            out = msm.run(gpu, base_buf, gpu.buffer(s))
+            got = affine_words(xyzz_to_affine(gpu.read(out, 32)))
+            assert np.array_equal(got, msm_ref("G1", bases, s)), f"round {rnd}, scalar set {i}"
+
+
+def fuzz_case(gpu, seed):
+    rnd = np.random.default_rng(seed)
+    n = int([rnd.integers(1, 64), rnd.integers(1, 1500), rnd.integers(1, 6000)][rnd.integers(0, 3)])
+    c = int(rnd.integers(9, 17))
+    item_points = int([1, 2, 5, 64, 1024][rnd.integers(0, 5)])
+    scalar_kind = int(rnd.integers(0, 5))
+    base_kind = int(rnd.integers(0, 3))
+    pool = random_points("G1", seed * 3 + 1, 4).reshape(4, 16)
+    fresh = random_points("G1", seed * 3 + 2, n).reshape(n, 16)
+    if base_kind == 0:
+        bases = fresh
+    elif base_kind == 1:
+        bases = pool[rnd.integers(0, 4, size=n)]
+    else:
+        bases = fresh.copy()
+        bases[rnd.random(n) < 0.1] = 0
+    if scalar_kind == 0:
+        s = random_fr(seed * 3 + 3, n)
+    elif scalar_kind == 1:
+        s = fr_words(int(v) for v in rnd.integers(0, 16, size=n))
+    elif scalar_kind == 2:
+        s = random_fr(seed * 3 + 3, n).reshape(n, 8)
+        s[rnd.random(n) < 0.9] = 0
+        s = s.reshape(-1)
+    elif scalar_kind == 3:
+        s = fr_words(int(v) for v in rnd.integers(0, 1 << 63, size=n, dtype=np.uint64))
+    else:
+        s = fr_words([0, 1, R - 1][int(v)] for v in rnd.integers(0, 3, size=n))
+    bases = np.ascontiguousarray(bases.reshape(-1))
+    got = gpu_msm(gpu, bases, s, (c, item_points))
+    assert np.array_equal(got, msm_ref("G1", bases, s)), (
+        f"FUZZ FAILURE: rerun with ZK_GPU_FUZZ_SEED={seed} (n={n}, c={c}, item_points={item_points}, "
+        f"scalars={scalar_kind}, bases={base_kind})")
+
+
+def test_fuzz(gpu):
+    if "ZK_GPU_FUZZ_SEED" in os.environ:
+        return fuzz_case(gpu, int(os.environ["ZK_GPU_FUZZ_SEED"]))
+    iters = int(os.environ.get("ZK_GPU_FUZZ_ITERS", 20 if quick() else 100))
+    for seed in range(1000, 1000 + iters):
+        fuzz_case(gpu, seed)
+
+
+# ---------------------------------------------------------------- full sizes
+
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0):
+    """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
+    uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G."""
+    n = 1 << log_n
+    k = uniform_scalars(n, 1000 + log_n + seed).reshape(n, 8)
+    k[infinity_mask(n, inf_fraction, log_n + seed)] = 0
+    k = k.reshape(-1)
+    dev = generator_multiples(gpu, Group.G1, k)
+    plain = gpu.read(dev, n * 16)
+    dev.free()
+    s = scalar_distribution(n, kind, 2000 + log_n + seed)
+    c = c or Msm.default_window(n)
+    base_buf = Msm.upload_bases(gpu, plain)
+    msm = Msm(gpu, n, c)
+    got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, gpu.buffer(s)), 32)))
+    gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
+    want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
+    assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}) wrong"
+    # spot check the device-built bases against the CPU
+    for i in (0, 1, n - 1):
+        assert np.array_equal(plain[16 * i: 16 * i + 16], cpu.generator_multiples("G1", k[8 * i: 8 * i + 8]))
+
+
+@pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"])
+@pytest.mark.parametrize("log_n", [18, 20, 22])
+def test_full_size_distributions(gpu, log_n, kind):
+    full_size_case(gpu, log_n, kind)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"] if not quick() else ["uniform"])
+def test_full_size_2_24(gpu, kind):
+    full_size_case(gpu, 24, kind)
+
+
+def test_full_size_other_window(gpu):
+    full_size_case(gpu, 20, "uniform", c=13)
+    full_size_case(gpu, 20, "r-1", c=18)

@@ -1,0 +1,125 @@
+"""NTT against the oracle and its mathematical properties (tests/ntt.rs:9-34,
+tests/properties.rs:25-138), plus the full benchmark sizes through size-independent checks."""
+import numpy as np
+import pytest
+
+from common import fr_words, gpu_ntt, quick, random_fr
+from oracle import bn254, cpu
+from zk_gpu import Ntt
+
+pytestmark = pytest.mark.gpu
+R = bn254.R
+
+
+@pytest.mark.parametrize("log_n", [10, 11, 12, 13, 14, 16, 18, 20, 22])
+def test_matches_oracle(gpu, log_n):
+    x = random_fr(100 + log_n, 1 << log_n)
+    ntt = Ntt(gpu, log_n)
+    buf = gpu.buffer(x)
+    ntt.forward(gpu, buf)
+    got = gpu.read(buf, x.size)
+    assert np.array_equal(got, cpu.ntt(x)), f"forward NTT mismatch at log_n={log_n}"
+    ntt.inverse(gpu, buf)
+    assert np.array_equal(gpu.read(buf, x.size), x), f"inverse NTT did not restore the input at log_n={log_n}"
+
+
+@pytest.mark.parametrize("log_n", [24, 26] if not quick() else [24])
+def test_full_size_round_trip_and_samples(gpu, log_n):
+    """At the benchmark sizes: forward equals the O(n) evaluation of sampled outputs, and
+    inverse(forward(x)) == x bit for bit."""
+    n = 1 << log_n
+    x = random_fr(7 + log_n, n)
+    ntt = Ntt(gpu, log_n)
+    buf = gpu.buffer(x)
+    ntt.forward(gpu, buf)
+    y = gpu.read(buf, x.size)
+    rnd = np.random.default_rng(log_n)
+    for k in [0, 1, n - 1] + [int(v) for v in rnd.integers(0, n, size=3)]:
+        assert np.array_equal(y[8 * k: 8 * k + 8], cpu.ntt_eval(x, k)), f"X[{k}] wrong at log_n={log_n}"
+    ntt.inverse(gpu, buf)
+    assert np.array_equal(gpu.read(buf, x.size), x)
+    # inverse sampled too
+    for k in [0, 5]:
+        assert np.array_equal(cpu.ntt_eval(y, k, inverse=True), x[8 * k: 8 * k + 8])
+
+
+def test_delta_is_a_power_sequence(gpu):
+    for log_n in (10, 11, 13):
+        n = 1 << log_n
+        ntt = Ntt(gpu, log_n)
+        w = bn254.root_of_unity(log_n)
+        for k in [0, 1, 2, 511, 512, n - 1]:
+            delta = np.zeros(8 * n, dtype=np.uint32)
+            delta[8 * k] = 1
+            want = fr_words(pow(w, j * k, R) for j in range(n))
+            assert np.array_equal(gpu_ntt(gpu, ntt, delta), want), f"NTT of delta_{k} wrong at log_n={log_n}"
+        c = 123456789
+        want = np.zeros(8 * n, dtype=np.uint32)
+        want[:8] = bn254.words32(c * n % R)
+        assert np.array_equal(gpu_ntt(gpu, ntt, fr_words([c] * n)), want)
+
+
+def test_is_linear(gpu):
+    for log_n in (10, 12, 14):
+        n = 1 << log_n
+        ntt = Ntt(gpu, log_n)
+        a, b = random_fr(1, n), random_fr(2, n)
+        c = 0x1234567890ABCDEF1234567
+        av = [bn254.from_words32(a[8 * i: 8 * i + 8]) for i in range(n)]
+        bv = [bn254.from_words32(b[8 * i: 8 * i + 8]) for i in range(n)]
+        comb = fr_words((x * c + y) % R for x, y in zip(av, bv))
+        fa, fb = gpu_ntt(gpu, ntt, a), gpu_ntt(gpu, ntt, b)
+        fav = [bn254.from_words32(fa[8 * i: 8 * i + 8]) for i in range(n)]
+        fbv = [bn254.from_words32(fb[8 * i: 8 * i + 8]) for i in range(n)]
+        want = fr_words((x * c + y) % R for x, y in zip(fav, fbv))
+        assert np.array_equal(gpu_ntt(gpu, ntt, comb), want), f"linearity failed at log_n={log_n}"
+
+
+def test_convolution_theorem(gpu):
+    n = 1 << 10
+    ntt = Ntt(gpu, 10)
+    a, b = random_fr(3, n), random_fr(4, n)
+    av = [bn254.from_words32(a[8 * i: 8 * i + 8]) for i in range(n)]
+    bv = [bn254.from_words32(b[8 * i: 8 * i + 8]) for i in range(n)]
+    expected = [0] * n
+    for i, x in enumerate(av):
+        if x:
+            for j, y in enumerate(bv):
+                expected[(i + j) % n] += x * y
+    expected = fr_words(v % R for v in expected)
+    fa, fb = gpu_ntt(gpu, ntt, a), gpu_ntt(gpu, ntt, b)
+    prod = fr_words(bn254.from_words32(fa[8 * i: 8 * i + 8]) * bn254.from_words32(fb[8 * i: 8 * i + 8]) % R
+                    for i in range(n))
+    assert np.array_equal(gpu_ntt(gpu, ntt, prod, inverse=True), expected), "convolution theorem failed"
+
+
+def test_round_trips_in_both_directions(gpu):
+    for log_n in (10, 15, 18):
+        ntt = Ntt(gpu, log_n)
+        x = random_fr(5 + log_n, 1 << log_n)
+        assert np.array_equal(gpu_ntt(gpu, ntt, gpu_ntt(gpu, ntt, x), inverse=True), x)
+        assert np.array_equal(gpu_ntt(gpu, ntt, gpu_ntt(gpu, ntt, x, inverse=True)), x)
+
+
+def test_extreme_values(gpu):
+    log_n = 12
+    n = 1 << log_n
+    ntt = Ntt(gpu, log_n)
+    rnd = np.random.default_rng(4)
+    mixed = fr_words([0, 1, R - 1][int(i)] for i in rnd.integers(0, 3, size=n))
+    for name, inp in [("zeros", fr_words([0] * n)), ("ones", fr_words([1] * n)), ("r-1", fr_words([R - 1] * n)),
+                      ("mixed", mixed)]:
+        got = gpu_ntt(gpu, ntt, inp)
+        assert np.array_equal(got, cpu.ntt(inp)), f"extreme input '{name}' wrong"
+        assert np.array_equal(gpu_ntt(gpu, ntt, got, inverse=True), inp), f"'{name}' does not round-trip"
+
+
+def test_plan_can_be_reused(gpu):
+    log_n = 13
+    n = 1 << log_n
+    ntt = Ntt(gpu, log_n)
+    inputs = [random_fr(50 + i, n) for i in range(4)]
+    first = [gpu_ntt(gpu, ntt, x) for x in inputs]
+    for i in reversed(range(4)):
+        assert np.array_equal(gpu_ntt(gpu, ntt, inputs[i]), first[i]), f"second run of input {i} differs"
+    assert np.array_equal(gpu_ntt(gpu, Ntt(gpu, log_n), inputs[0]), first[0])

@@ -1,0 +1,444 @@
+// extern "C" entry points of include/zkg.h: argument checks, exception -> status code, and the
+// thread-local error message. Every function here is a thin shell over the plans.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "host_field.hpp"
+#include "msm.hpp"
+#include "ntt.hpp"
+#include "runtime.hpp"
+#include "testing.hpp"
+
+namespace zkg {
+
+std::atomic<uint64_t> g_launches{0};
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+const std::string& last_error() { return g_last_error; }
+
+template <class Fn>
+static int guard(Fn&& fn) {
+  try {
+    fn();
+    return ZKG_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return ZKG_ENOMEM;
+  } catch (...) {
+    set_error("unexpected internal error");
+    return ZKG_ECUDA;
+  }
+}
+
+static void need(const void* p, const char* what) {
+  if (!p) fail(ZKG_EINVAL, std::string(what) + " is NULL");
+}
+
+static zkg_buf* new_buffer(zkg_ctx* ctx, size_t words) {
+  zkg_buf* b = new zkg_buf;
+  b->ctx = ctx;
+  b->words = words;
+  try {
+    b->ptr = device_alloc(words * 4, "buffer");
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  return b;
+}
+
+static void copy_in(zkg_ctx* ctx, uint32_t* dst, const uint32_t* src, size_t words) {
+  if (words == 0) return;
+  check_cuda(cudaMemcpyAsync(dst, src, words * 4, cudaMemcpyHostToDevice, ctx->stream), "host to device copy");
+  // From pageable memory the copy has consumed the host array when the call returns; from
+  // page-locked memory it may still be in flight, so wait for it.
+  if (is_pinned(src)) check_cuda(cudaStreamSynchronize(ctx->stream), "host to device copy");
+}
+
+}  // namespace zkg
+
+using namespace zkg;
+
+extern "C" {
+
+const char* zkg_last_error(void) { return g_last_error.c_str(); }
+
+int zkg_ctx_new(int device, zkg_ctx** out) {
+  return guard([&] {
+    need(out, "out");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      fail(ZKG_ENODEV, std::string("no GPU adapter: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "no CUDA device"));
+    }
+    if (device < 0 || device >= count) fail(ZKG_ENODEV, "no GPU adapter: device index out of range");
+    zkg_ctx* ctx = new zkg_ctx;
+    ctx->device = device;
+    try {
+      check_cuda(cudaSetDevice(device), "cudaSetDevice");
+      cudaDeviceProp prop;
+      check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+      ctx->sm_count = prop.multiProcessorCount;
+      std::strncpy(ctx->name, prop.name, sizeof(ctx->name) - 1);
+      check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    } catch (...) {
+      delete ctx;
+      throw;
+    }
+    *out = ctx;
+  });
+}
+
+void zkg_ctx_free(zkg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+}
+
+int zkg_ctx_sync(zkg_ctx* ctx) {
+  return guard([&] {
+    need(ctx, "ctx");
+    use(ctx);
+    check_cuda(cudaStreamSynchronize(ctx->stream), "device work");
+    check_cuda(cudaGetLastError(), "device work");
+  });
+}
+
+int zkg_ctx_device_name(zkg_ctx* ctx, char* out, size_t cap) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    if (cap == 0) return;
+    std::strncpy(out, ctx->name, cap - 1);
+    out[cap - 1] = 0;
+  });
+}
+
+int zkg_buf_new(zkg_ctx* ctx, const uint32_t* data, size_t words, zkg_buf** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    if (words) need(data, "data");
+    use(ctx);
+    zkg_buf* b = new_buffer(ctx, words);
+    try {
+      copy_in(ctx, b->ptr, data, words);
+    } catch (...) {
+      zkg_buf_free(b);
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int zkg_buf_zeroed(zkg_ctx* ctx, size_t words, zkg_buf** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    use(ctx);
+    zkg_buf* b = new_buffer(ctx, words);
+    try {
+      check_cuda(cudaMemsetAsync(b->ptr, 0, words * 4, ctx->stream), "buffer clear");
+    } catch (...) {
+      zkg_buf_free(b);
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int zkg_buf_write(zkg_ctx* ctx, zkg_buf* buf, size_t offset_words, const uint32_t* data, size_t words) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(buf, "buf");
+    if (words) need(data, "data");
+    if (offset_words > buf->words || words > buf->words - offset_words)
+      fail(ZKG_ESIZE, "write of " + std::to_string(words) + " words at offset " + std::to_string(offset_words) +
+                          " overruns a buffer of " + std::to_string(buf->words) + " words");
+    use(ctx);
+    copy_in(ctx, buf->ptr + offset_words, data, words);
+  });
+}
+
+int zkg_buf_read(zkg_ctx* ctx, const zkg_buf* buf, uint32_t* out, size_t words) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(buf, "buf");
+    if (words) need(out, "out");
+    if (words > buf->words)
+      fail(ZKG_ESIZE, "read of " + std::to_string(words) + " words from a buffer of " + std::to_string(buf->words));
+    use(ctx);
+    if (words)
+      check_cuda(cudaMemcpyAsync(out, buf->ptr, words * 4, cudaMemcpyDeviceToHost, ctx->stream), "device to host copy");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "GPU read failed");
+  });
+}
+
+size_t zkg_buf_words(const zkg_buf* buf) { return buf ? buf->words : 0; }
+void* zkg_buf_device_ptr(const zkg_buf* buf) { return buf ? buf->ptr : nullptr; }
+
+void zkg_buf_free(zkg_buf* buf) {
+  if (!buf || !buf->owned) return;
+  if (buf->ctx) cudaSetDevice(buf->ctx->device);
+  if (buf->ptr) cudaFree(buf->ptr);
+  delete buf;
+}
+
+uint32_t zkg_msm_default_window(size_t n) { return default_window(n); }
+
+static int upload(zkg_ctx* ctx, const uint32_t* xy, size_t words, bool mont256, zkg_buf** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    if (words) need(xy, "xy");
+    if (words % 8) fail(ZKG_EINVAL, "bases hold whole 8-word coordinates");
+    use(ctx);
+    zkg_buf* b = new_buffer(ctx, words);
+    try {
+      copy_in(ctx, b->ptr, xy, words);
+      upload_bases(ctx, xy, words, mont256, b);
+    } catch (...) {
+      zkg_buf_free(b);
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int zkg_msm_upload_bases(zkg_ctx* ctx, const uint32_t* plain_xy, size_t words, zkg_buf** out) {
+  return upload(ctx, plain_xy, words, false, out);
+}
+
+int zkg_msm_upload_bases_montgomery_256(zkg_ctx* ctx, const uint32_t* xy, size_t words, zkg_buf** out) {
+  return upload(ctx, xy, words, true, out);
+}
+
+int zkg_msm_new(zkg_ctx* ctx, int group, size_t n, uint32_t c, uint32_t item_points, zkg_msm** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    *out = nullptr;
+    *out = new zkg_msm(ctx, group, n, c, item_points);
+  });
+}
+
+void zkg_msm_free(zkg_msm* msm) {
+  if (!msm) return;
+  cudaSetDevice(msm->plan.ctx->device);
+  cudaStreamSynchronize(msm->plan.ctx->stream);
+  delete msm;
+}
+
+int zkg_msm_group(const zkg_msm* msm) { return msm ? msm->plan.group : 0; }
+
+int zkg_msm_run(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, const zkg_buf** result) {
+  return guard([&] {
+    need(msm, "msm");
+    need(bases, "bases");
+    need(scalars, "scalars");
+    msm->plan.run(bases, scalars);
+    if (result) *result = &msm->plan.result_handle;
+  });
+}
+
+int zkg_msm_profile(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, zkg_stage_time* out, size_t cap,
+                    size_t* count) {
+  return guard([&] {
+    need(msm, "msm");
+    need(bases, "bases");
+    need(scalars, "scalars");
+    auto times = msm->plan.profile(bases, scalars);
+    size_t k = 0;
+    for (auto& t : times) {
+      if (k >= cap || !out) break;
+      std::memset(out[k].stage, 0, sizeof(out[k].stage));
+      std::strncpy(out[k].stage, t.first.c_str(), sizeof(out[k].stage) - 1);
+      out[k].ms = t.second;
+      k++;
+    }
+    if (count) *count = k;
+  });
+}
+
+int zkg_xyzz_to_affine(const uint32_t* words, uint64_t* x, uint64_t* y) {
+  if (!words || !x || !y) {
+    set_error("NULL argument");
+    return -ZKG_EINVAL;
+  }
+  const host::Field& f = host::fq();
+  host::U256 X = host::from_words32(words), Y = host::from_words32(words + 8);
+  host::U256 ZZ = host::from_words32(words + 16), ZZZ = host::from_words32(words + 24);
+  if (host::is_zero(ZZ)) {
+    std::memset(x, 0, 32);
+    std::memset(y, 0, 32);
+    return 0;
+  }
+  host::U256 ax = host::from_mont(host::mul(X, host::inverse(ZZ, f), f), f);
+  host::U256 ay = host::from_mont(host::mul(Y, host::inverse(ZZZ, f), f), f);
+  std::memcpy(x, ax.v, 32);
+  std::memcpy(y, ay.v, 32);
+  return 1;
+}
+
+int zkg_xyzz_to_affine_g2(const uint32_t* words, uint64_t* x, uint64_t* y) {
+  if (!words || !x || !y) {
+    set_error("NULL argument");
+    return -ZKG_EINVAL;
+  }
+  const host::Field& f = host::fq();
+  auto fq2 = [&](int i) { return host::U512{host::from_words32(words + 16 * i), host::from_words32(words + 16 * i + 8)}; };
+  host::U512 X = fq2(0), Y = fq2(1), ZZ = fq2(2), ZZZ = fq2(3);
+  if (host::is_zero(ZZ.a) && host::is_zero(ZZ.b)) {
+    std::memset(x, 0, 64);
+    std::memset(y, 0, 64);
+    return 0;
+  }
+  host::U512 ax = host::fq2_mul(X, host::fq2_inverse(ZZ));
+  host::U512 ay = host::fq2_mul(Y, host::fq2_inverse(ZZZ));
+  host::U256 outs[4] = {host::from_mont(ax.a, f), host::from_mont(ax.b, f), host::from_mont(ay.a, f),
+                        host::from_mont(ay.b, f)};
+  std::memcpy(x, outs[0].v, 32);
+  std::memcpy(x + 4, outs[1].v, 32);
+  std::memcpy(y, outs[2].v, 32);
+  std::memcpy(y + 4, outs[3].v, 32);
+  return 1;
+}
+
+int zkg_ntt_new(zkg_ctx* ctx, uint32_t log_n, zkg_ntt** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    *out = nullptr;
+    *out = new zkg_ntt(ctx, log_n);
+  });
+}
+
+void zkg_ntt_free(zkg_ntt* ntt) {
+  if (!ntt) return;
+  cudaSetDevice(ntt->plan.ctx->device);
+  cudaStreamSynchronize(ntt->plan.ctx->stream);
+  delete ntt;
+}
+
+uint32_t zkg_ntt_log_n(const zkg_ntt* ntt) { return ntt ? ntt->plan.log_n : 0; }
+
+int zkg_ntt_forward(zkg_ntt* ntt, zkg_buf* data) {
+  return guard([&] {
+    need(ntt, "ntt");
+    need(data, "data");
+    ntt->plan.run(data, false);
+  });
+}
+
+int zkg_ntt_inverse(zkg_ntt* ntt, zkg_buf* data) {
+  return guard([&] {
+    need(ntt, "ntt");
+    need(data, "data");
+    ntt->plan.run(data, true);
+  });
+}
+
+void* zkg_ctx_stream(zkg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+uint64_t zkg_launch_count(void) { return g_launches.load(); }
+
+int zkg_host_alloc(size_t bytes, void** out) {
+  return guard([&] {
+    need(out, "out");
+    *out = nullptr;
+    check_cuda(cudaHostAlloc(out, bytes ? bytes : 16, cudaHostAllocDefault), "cudaHostAlloc");
+  });
+}
+
+void zkg_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+static void write_times(const std::vector<double>& ms, const std::vector<std::string>& names, zkg_stage_time* out,
+                        size_t cap, size_t* count) {
+  size_t k = 0;
+  for (size_t i = 0; i < ms.size() && k < cap && out; i++, k++) {
+    std::memset(out[k].stage, 0, sizeof(out[k].stage));
+    std::strncpy(out[k].stage, names[i].c_str(), sizeof(out[k].stage) - 1);
+    out[k].ms = ms[i];
+  }
+  if (count) *count = k;
+}
+
+int zkg_msm_set_timing(zkg_msm* msm, int enable) {
+  return guard([&] {
+    need(msm, "msm");
+    msm->plan.timer.enabled = enable != 0;
+  });
+}
+
+int zkg_msm_stage_times(zkg_msm* msm, zkg_stage_time* out, size_t cap, size_t* count, size_t* runs) {
+  return guard([&] {
+    need(msm, "msm");
+    use(msm->plan.ctx);
+    std::vector<double> ms = msm->plan.timer.collect(MsmPlan::kStages, runs);
+    std::vector<std::string> names;
+    for (int i = 0; i < MsmPlan::kStages; i++) names.push_back(MsmPlan::stage_name(i));
+    write_times(ms, names, out, cap, count);
+  });
+}
+
+int zkg_ntt_set_timing(zkg_ntt* ntt, int enable) {
+  return guard([&] {
+    need(ntt, "ntt");
+    ntt->plan.timer.enabled = enable != 0;
+  });
+}
+
+int zkg_ntt_pass_times(zkg_ntt* ntt, zkg_stage_time* out, size_t cap, size_t* count, size_t* runs) {
+  return guard([&] {
+    need(ntt, "ntt");
+    use(ntt->plan.ctx);
+    int np = (int)ntt->plan.passes.size();
+    std::vector<double> ms = ntt->plan.timer.collect(np, runs);
+    std::vector<std::string> names;
+    for (int i = 0; i < np; i++) names.push_back("pass " + std::to_string(i));
+    write_times(ms, names, out, cap, count);
+  });
+}
+
+int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(ops_per_second, "ops_per_second");
+    if (variant < 0 || variant > 3) fail(ZKG_EINVAL, "variant must be 0..3");
+    *ops_per_second = bench_integer_pipe(ctx, variant);
+  });
+}
+
+int zkg_test_point_ops(zkg_ctx* ctx, int group, const uint32_t* pairs, size_t count, uint32_t* out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(pairs, "pairs");
+    need(out, "out");
+    if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+    if (count) point_ops(ctx, group, pairs, count, out);
+  });
+}
+
+int zkg_generator_multiples(zkg_ctx* ctx, int group, const zkg_buf* scalars, size_t n, int mont256, zkg_buf* out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(scalars, "scalars");
+    need(out, "out");
+    if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+    if (n) generator_multiples(ctx, group, scalars, n, mont256, out);
+  });
+}
+
+}  // extern "C"

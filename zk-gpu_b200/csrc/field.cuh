@@ -1,0 +1,337 @@
+// BN254 base field Fq and scalar field Fr on sm_100a: 8 x 32-bit limbs, Montgomery radix
+// R = 2^256, products on the integer multiply-add pipe through PTX carry chains
+// (mad.lo.cc / madc.hi.cc). No tensor cores: this is exact modular integer arithmetic.
+//
+// Replaces the reference's generated WGSL field code (src/field.rs:55-181: 20 x 13-bit limbs,
+// R = 2^260, deferred carries). Memory format is unchanged: 8 little-endian u32 words per
+// element (src/field.rs:63-93). Values in registers and in memory are always fully reduced
+// (< p), so equality and zero tests are word compares.
+#pragma once
+#include <cstdint>
+
+namespace zkg {
+
+// Modulus parameters. INV = -p^-1 mod 2^32; ONE = 2^256 mod p (Montgomery one);
+// R2 = 2^512 mod p (to_montgomery multiplier).
+struct FqParams {
+  static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u;
+  static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t INV = 0xe4866389u;
+  static constexpr uint32_t ONE0 = 0xc58f0d9du, ONE1 = 0xd35d438du, ONE2 = 0xf5c70b3du, ONE3 = 0x0a78eb28u;
+  static constexpr uint32_t ONE4 = 0x7879462cu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+};
+
+struct FrParams {
+  static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u;
+  static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t INV = 0xefffffffu;
+  static constexpr uint32_t ONE0 = 0x4ffffffbu, ONE1 = 0xac96341cu, ONE2 = 0x9f60cd29u, ONE3 = 0x36fc7695u;
+  static constexpr uint32_t ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+};
+
+template <class P>
+struct Fp {
+  uint32_t w[8];
+
+  __device__ __forceinline__ static Fp zero() {
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.w[i] = 0;
+    return r;
+  }
+  __device__ __forceinline__ static Fp one() {
+    Fp r;
+    r.w[0] = P::ONE0; r.w[1] = P::ONE1; r.w[2] = P::ONE2; r.w[3] = P::ONE3;
+    r.w[4] = P::ONE4; r.w[5] = P::ONE5; r.w[6] = P::ONE6; r.w[7] = P::ONE7;
+    return r;
+  }
+  __device__ __forceinline__ bool is_zero() const {
+    uint32_t x = w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7];
+    return x == 0;
+  }
+  __device__ __forceinline__ bool operator==(const Fp& o) const {
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) x |= w[i] ^ o.w[i];
+    return x == 0;
+  }
+  __device__ __forceinline__ bool operator!=(const Fp& o) const { return !(*this == o); }
+};
+
+using Fq = Fp<FqParams>;
+using Fr = Fp<FrParams>;
+
+// ------------------------------------------------------------------ add / sub
+
+// r = a + b mod p. Both < p < 2^254, so a + b < 2^255 never carries out of 8 words.
+template <class P>
+__device__ __forceinline__ Fp<P> operator+(const Fp<P>& a, const Fp<P>& b) {
+  Fp<P> s, d;
+  uint32_t borrow;
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=&r"(s.w[0]), "=&r"(s.w[1]), "=&r"(s.w[2]), "=&r"(s.w[3]), "=&r"(s.w[4]), "=&r"(s.w[5]), "=&r"(s.w[6]),
+        "=&r"(s.w[7])
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(a.w[4]), "r"(a.w[5]), "r"(a.w[6]), "r"(a.w[7]),
+        "r"(b.w[0]), "r"(b.w[1]), "r"(b.w[2]), "r"(b.w[3]), "r"(b.w[4]), "r"(b.w[5]), "r"(b.w[6]), "r"(b.w[7]));
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
+        "=&r"(d.w[7]), "=&r"(borrow)
+      : "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7]),
+        "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
+  // borrow = 0xffffffff when s < p: keep s; otherwise take s - p.
+  Fp<P> r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
+  return r;
+}
+
+// r = a - b mod p: subtract, then add p back under the borrow mask.
+template <class P>
+__device__ __forceinline__ Fp<P> operator-(const Fp<P>& a, const Fp<P>& b) {
+  Fp<P> d, r;
+  uint32_t borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
+        "=&r"(d.w[7]), "=&r"(borrow)
+      : "r"(a.w[0]), "r"(a.w[1]), "r"(a.w[2]), "r"(a.w[3]), "r"(a.w[4]), "r"(a.w[5]), "r"(a.w[6]), "r"(a.w[7]),
+        "r"(b.w[0]), "r"(b.w[1]), "r"(b.w[2]), "r"(b.w[3]), "r"(b.w[4]), "r"(b.w[5]), "r"(b.w[6]), "r"(b.w[7]));
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=&r"(r.w[0]), "=&r"(r.w[1]), "=&r"(r.w[2]), "=&r"(r.w[3]), "=&r"(r.w[4]), "=&r"(r.w[5]), "=&r"(r.w[6]),
+        "=&r"(r.w[7])
+      : "r"(d.w[0]), "r"(d.w[1]), "r"(d.w[2]), "r"(d.w[3]), "r"(d.w[4]), "r"(d.w[5]), "r"(d.w[6]), "r"(d.w[7]),
+        "r"(P::P0 & borrow), "r"(P::P1 & borrow), "r"(P::P2 & borrow), "r"(P::P3 & borrow), "r"(P::P4 & borrow),
+        "r"(P::P5 & borrow), "r"(P::P6 & borrow), "r"(P::P7 & borrow));
+  return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> neg(const Fp<P>& a) {
+  return Fp<P>::zero() - a;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> dbl(const Fp<P>& a) {
+  return a + a;
+}
+
+// ------------------------------------------------------------------ Montgomery product
+
+// t[i..i+8] += a * bi. t[i+8] is fresh (never written before this row) and is set from the
+// carry of the low-half chain. Low halves land on t[i..i+7], high halves on t[i+1..i+8].
+#define ZKG_MAD_ROW(t, i, a, bi)                                                                  \
+  asm("mad.lo.cc.u32  %0, %9, %17, %0;\n\t"                                                        \
+      "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                       \
+      "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                       \
+      "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                       \
+      "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                       \
+      "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                       \
+      "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                       \
+      "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                       \
+      "addc.u32       %8, 0, 0;\n\t"                                                               \
+      "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"                                                        \
+      "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                       \
+      "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                       \
+      "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                       \
+      "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                       \
+      "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                       \
+      "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                       \
+      "madc.hi.u32    %8, %16, %17, %8;"                                                           \
+      : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]), "+r"(t[i + 5]), \
+        "+r"(t[i + 6]), "+r"(t[i + 7]), "=&r"(t[i + 8])                                              \
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(bi))
+
+// t[i..i+8] += m * p with m = t[i] * INV, which clears t[i]. The value stays below 2^288
+// because p < 2^254 (no carry out of t[i+8]).
+#define ZKG_RED_ROW(P, t, i)                                                                       \
+  do {                                                                                             \
+    uint32_t m_ = t[i] * P::INV;                                                                   \
+    asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                                      \
+        "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                                      \
+        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                      \
+        "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                                      \
+        "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                                      \
+        "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                                      \
+        "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                                      \
+        "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                                      \
+        "addc.u32       %8, %8, 0;\n\t"                                                            \
+        "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                                      \
+        "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                                      \
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                      \
+        "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                                      \
+        "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                                      \
+        "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                                      \
+        "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                                      \
+        "madc.hi.u32    %8, %9, %17, %8;"                                                          \
+        : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]),              \
+          "+r"(t[i + 5]), "+r"(t[i + 6]), "+r"(t[i + 7]), "+r"(t[i + 8])                           \
+        : "r"(m_), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5),        \
+          "n"(P::P6), "n"(P::P7));                                                                 \
+  } while (0)
+
+// Returns a * b * 2^-256 mod p (coarsely integrated operand scanning: one product row, then
+// one reduction row, per limb of b; 33 multiply-adds per limb).
+template <class P>
+__device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
+  uint32_t t[17];
+#pragma unroll
+  for (int i = 0; i < 8; i++) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    ZKG_MAD_ROW(t, i, a.w, b.w[i]);
+    ZKG_RED_ROW(P, t, i);
+  }
+  // t[8..15] < 2p: one conditional subtraction.
+  Fp<P> s, d;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s.w[i] = t[8 + i];
+  uint32_t borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
+        "=&r"(d.w[7]), "=&r"(borrow)
+      : "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7]),
+        "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
+  Fp<P> r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
+  return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> sqr(const Fp<P>& a) {
+  return a * a;
+}
+
+// ------------------------------------------------------------------ memory helpers
+
+// 32-byte element loads/stores as two 16-byte vector accesses (the address must be 16-byte
+// aligned; every buffer and element offset in this library is).
+template <class F>
+__device__ __forceinline__ F load_fe(const void* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 lo = q[0], hi = q[1];
+  F r;
+  r.w[0] = lo.x; r.w[1] = lo.y; r.w[2] = lo.z; r.w[3] = lo.w;
+  r.w[4] = hi.x; r.w[5] = hi.y; r.w[6] = hi.z; r.w[7] = hi.w;
+  return r;
+}
+
+template <class F>
+__device__ __forceinline__ F load_fe_cg(const void* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 lo = __ldcg(q), hi = __ldcg(q + 1);
+  F r;
+  r.w[0] = lo.x; r.w[1] = lo.y; r.w[2] = lo.z; r.w[3] = lo.w;
+  r.w[4] = hi.x; r.w[5] = hi.y; r.w[6] = hi.z; r.w[7] = hi.w;
+  return r;
+}
+
+template <class F>
+__device__ __forceinline__ void store_fe(void* p, const F& a) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+  q[0] = make_uint4(a.w[0], a.w[1], a.w[2], a.w[3]);
+  q[1] = make_uint4(a.w[4], a.w[5], a.w[6], a.w[7]);
+}
+
+// ------------------------------------------------------------------ Fq2 = Fq[u] / (u^2 + 1)
+
+// a + b*u. Karatsuba product in three Fq products, square in two (the reference's G2 prelude,
+// src/group.rs:38-48).
+struct Fq2 {
+  Fq a, b;
+  __device__ __forceinline__ static Fq2 zero() { return Fq2{Fq::zero(), Fq::zero()}; }
+  __device__ __forceinline__ static Fq2 one() { return Fq2{Fq::one(), Fq::zero()}; }
+  __device__ __forceinline__ bool is_zero() const { return a.is_zero() && b.is_zero(); }
+  __device__ __forceinline__ bool operator==(const Fq2& o) const { return a == o.a && b == o.b; }
+};
+
+__device__ __forceinline__ Fq2 operator+(const Fq2& x, const Fq2& y) { return Fq2{x.a + y.a, x.b + y.b}; }
+__device__ __forceinline__ Fq2 operator-(const Fq2& x, const Fq2& y) { return Fq2{x.a - y.a, x.b - y.b}; }
+__device__ __forceinline__ Fq2 neg(const Fq2& x) { return Fq2{neg(x.a), neg(x.b)}; }
+__device__ __forceinline__ Fq2 dbl(const Fq2& x) { return Fq2{x.a + x.a, x.b + x.b}; }
+__device__ __forceinline__ Fq2 operator*(const Fq2& x, const Fq2& y) {
+  Fq ac = x.a * y.a;
+  Fq bd = x.b * y.b;
+  Fq cross = (x.a + x.b) * (y.a + y.b);
+  return Fq2{ac - bd, (cross - ac) - bd};
+}
+__device__ __forceinline__ Fq2 sqr(const Fq2& x) {
+  Fq ab = x.a * x.b;
+  return Fq2{(x.a + x.b) * (x.a - x.b), ab + ab};
+}
+
+template <class F>
+struct FieldWords;
+template <>
+struct FieldWords<Fq> {
+  static constexpr int value = 8;
+};
+template <>
+struct FieldWords<Fr> {
+  static constexpr int value = 8;
+};
+template <>
+struct FieldWords<Fq2> {
+  static constexpr int value = 16;
+};
+
+template <class F>
+__device__ __forceinline__ F load_elem(const uint32_t* p);
+template <>
+__device__ __forceinline__ Fq load_elem<Fq>(const uint32_t* p) {
+  return load_fe<Fq>(p);
+}
+template <>
+__device__ __forceinline__ Fr load_elem<Fr>(const uint32_t* p) {
+  return load_fe<Fr>(p);
+}
+template <>
+__device__ __forceinline__ Fq2 load_elem<Fq2>(const uint32_t* p) {
+  return Fq2{load_fe<Fq>(p), load_fe<Fq>(p + 8)};
+}
+
+__device__ __forceinline__ void store_elem(uint32_t* p, const Fq& x) { store_fe(p, x); }
+__device__ __forceinline__ void store_elem(uint32_t* p, const Fr& x) { store_fe(p, x); }
+__device__ __forceinline__ void store_elem(uint32_t* p, const Fq2& x) {
+  store_fe(p, x.a);
+  store_fe(p + 8, x.b);
+}
+
+}  // namespace zkg

@@ -1,0 +1,250 @@
+// MSM plan and driver: the host side of Msm (src/msm.rs:82-298), sm_100a kernels in
+// msm_kernels.cuh.
+//
+// A plan owns every scratch buffer for a fixed (group, n, c, L); runs are queued on the
+// context stream with no host synchronisation (data-dependent sizes such as the number of
+// nonzero digits stay on the device: kernels read them and exit early), so a plan can be
+// reused any number of times and captured in a CUDA graph.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host_field.hpp"
+#include "msm.hpp"
+#include "msm_kernels.cuh"
+
+namespace zkg {
+
+uint32_t default_window(size_t n) {
+  // clamp(log2(max(n,1)) - 5, 11, 16) (src/msm.rs:78-80)
+  size_t v = n < 1 ? 1 : n;
+  int lg = 63 - __builtin_clzll((unsigned long long)v);
+  int c = lg - 5;
+  if (c < 11) c = 11;
+  if (c > 16) c = 16;
+  return (uint32_t)c;
+}
+
+// Points accumulated per thread when the caller does not choose: about one wave of 1024
+// threads per SM over the whole sorted array, between 8 and 256 (a power of two).
+static uint32_t auto_seg_len(size_t n, uint32_t windows) {
+  double entries = (double)n * windows;
+  double target = entries / (148.0 * 1024.0);
+  uint32_t l = 8;
+  while (l < 256 && l < target) l <<= 1;
+  return l;
+}
+
+MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_points)
+    : ctx(c_), group(group_), n(n_), c(c) {
+  if (n < 1) fail(ZKG_EINVAL, "an MSM needs at least one point");
+  if (c < 9 || c > 20) fail(ZKG_EINVAL, "window size c must be in 9..=20, got " + std::to_string(c));
+  if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+  if (n >= (size_t)kNegBit) fail(ZKG_EINVAL, "an MSM holds fewer than 2^31 points");
+  windows = (255 + c - 1) / c;
+  half = 1u << (c - 1);
+  slots = (size_t)windows * half;
+  seg_len = item_points ? item_points : auto_seg_len(n, windows);
+  const size_t xw = xyzz_words();
+  const size_t max_entries = (size_t)windows * n;
+  if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
+
+  use(ctx);
+  counts.alloc(slots, "msm counts");
+  slot_start.alloc(slots + 1, "msm slot_start");
+  cursor.alloc(slots, "msm cursor");
+  scan_tiles_n = (uint32_t)((slots + kScanTile - 1) / kScanTile);
+  if (scan_tiles_n > (uint32_t)kScanTile) fail(ZKG_EINVAL, "too many bucket slots");
+  tile_sums.alloc(scan_tiles_n, "msm scan tiles");
+  sorted.alloc(max_entries, "msm sorted");
+  buckets.alloc(slots * xw, "msm buckets");
+
+  heads_max = (max_entries + seg_len - 1) / seg_len;
+  size_t len = heads_max;
+  merge_levels = 0;
+  while (len > 1) {
+    len = (len + kMergeFanIn - 1) / kMergeFanIn;
+    merge_levels++;
+  }
+  size_t second = (heads_max + kMergeFanIn - 1) / kMergeFanIn;
+  heads[0].alloc(heads_max * xw, "msm heads");
+  head_keys[0].alloc(heads_max, "msm head keys");
+  heads[1].alloc(std::max<size_t>(second, 1) * xw, "msm heads");
+  head_keys[1].alloc(std::max<size_t>(second, 1), "msm head keys");
+
+  // Running-sum levels: m_0 = B; m_{l+1} = ceil(m_l / 16) - 1 while positive.
+  std::memset(&levels, 0, sizeof(levels));
+  uint32_t m = half;
+  size_t tot_points = 0, run_points = 0;
+  std::vector<uint32_t> ms;
+  while (m > 0) {
+    if (levels.count >= (uint32_t)kMaxReduceLevels) fail(ZKG_EINVAL, "too many reduction levels");
+    uint32_t chunks = (m + kChunk - 1) / kChunk;
+    ms.push_back(m);
+    levels.tot_len[levels.count] = chunks;
+    levels.tot_offset[levels.count] = (uint32_t)tot_points;
+    tot_points += (size_t)chunks * windows;
+    m = chunks - 1;
+    levels.count++;
+    run_points = std::max<size_t>(run_points, (size_t)m * windows);
+  }
+  level_m = ms;
+  tots.alloc(tot_points * xw, "msm tots");
+  runs[0].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
+  runs[1].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
+  window_sums.alloc((size_t)windows * xw, "msm window sums");
+  result.alloc(xw, "msm result");
+  result_handle.ctx = ctx;
+  result_handle.ptr = result.ptr;
+  result_handle.words = xw;
+  result_handle.owned = false;
+  check_cuda(cudaMemsetAsync(result.ptr, 0, xw * 4, ctx->stream), "msm result init");
+}
+
+size_t MsmPlan::xyzz_words() const { return group == ZKG_G1 ? 32 : 64; }
+size_t MsmPlan::affine_words() const { return group == ZKG_G1 ? 16 : 32; }
+
+void MsmPlan::check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const {
+  // Msm::check_buffers (src/msm.rs:271-282): byte counts in the messages, like the reference.
+  size_t sb = scalars->words * 4, need_s = n * 32;
+  if (sb < need_s)
+    fail(ZKG_ESIZE, "scalars buffer holds " + std::to_string(sb) + " bytes; " + std::to_string(n) +
+                        " scalars need " + std::to_string(need_s));
+  size_t bb = bases->words * 4, need_b = n * affine_words() * 4;
+  if (bb < need_b)
+    fail(ZKG_ESIZE, "bases buffer holds " + std::to_string(bb) + " bytes; " + std::to_string(n) + " points need " +
+                        std::to_string(need_b));
+}
+
+template <class F>
+void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
+  const unsigned b256 = 256;
+  switch (which) {
+    case kStageCount:
+      check_cuda(cudaMemsetAsync(counts.ptr, 0, slots * 4, s), "msm counts clear");
+      msm_count<<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+      check_launch("msm_count");
+      break;
+    case kStageScan:
+      scan_tile_sums<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr);
+      check_launch("scan_tile_sums");
+      scan_tiles<<<1, kScanBlock, 0, s>>>(tile_sums.ptr, scan_tiles_n, slot_start.ptr + slots);
+      check_launch("scan_tiles");
+      scan_apply<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr, slot_start.ptr, cursor.ptr);
+      check_launch("scan_apply");
+      break;
+    case kStageScatter:
+      msm_scatter<<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
+      check_launch("msm_scatter");
+      break;
+    case kStageAccumulate:
+      msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr, (uint32_t)slots,
+                                                                 seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      check_launch("msm_accumulate");
+      break;
+    case kStageMerge: {
+      size_t len = heads_max;
+      for (uint32_t l = 0; l < merge_levels; l++) {
+        size_t out_len = (len + kMergeFanIn - 1) / kMergeFanIn;
+        int src = l & 1, dst = src ^ 1;
+        msm_merge<F><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)slots, seg_len, l,
+                                                            heads[src].ptr, head_keys[src].ptr, heads[dst].ptr,
+                                                            head_keys[dst].ptr, buckets.ptr);
+        check_launch("msm_merge");
+        len = out_len;
+      }
+      break;
+    }
+    case kStageReduce: {
+      const uint32_t* in = buckets.ptr;
+      uint32_t in_stride = half;
+      for (uint32_t l = 0; l < levels.count; l++) {
+        uint32_t m = level_m[l];
+        uint32_t chunks = (m + kChunk - 1) / kChunk;
+        uint32_t* run_out = runs[l & 1].ptr;
+        msm_reduce_level<F><<<grid_for((size_t)chunks * windows, 128), 128, 0, s>>>(
+            in, in_stride, m, windows, l == 0 ? slot_start.ptr : nullptr,
+            tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(), chunks, run_out, chunks > 1 ? chunks - 1 : 1);
+        check_launch("msm_reduce_level");
+        in = run_out;
+        in_stride = chunks > 1 ? chunks - 1 : 1;
+      }
+      break;
+    }
+    case kStageWindows:
+      msm_window_sums<F><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<F>), s>>>(tots.ptr, levels,
+                                                                                          window_sums.ptr);
+      check_launch("msm_window_sums");
+      break;
+    case kStageCombine:
+      msm_combine<F><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      check_launch("msm_combine");
+      break;
+  }
+}
+
+const char* MsmPlan::stage_name(int which) {
+  static const char* names[kStages] = {"count", "scan", "scatter", "accumulate", "merge", "reduce", "window sums", "combine"};
+  return names[which];
+}
+
+void MsmPlan::enqueue(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
+  for (int st = 0; st < kStages; st++) {
+    size_t ev = timer.enabled ? timer.begin(st, s) : 0;
+    if (group == ZKG_G1) stage<Fq>(st, bases, scalars, s);
+    else stage<Fq2>(st, bases, scalars, s);
+    if (timer.enabled) timer.end(ev, s);
+  }
+  if (timer.enabled) timer.runs++;
+}
+
+void MsmPlan::run(const zkg_buf* bases, const zkg_buf* scalars) {
+  check_buffers(bases, scalars);
+  use(ctx);
+  enqueue(bases->ptr, scalars->ptr, ctx->stream);
+}
+
+std::vector<std::pair<std::string, double>> MsmPlan::profile(const zkg_buf* bases, const zkg_buf* scalars) {
+  check_buffers(bases, scalars);
+  use(ctx);
+  std::vector<std::pair<std::string, double>> out;
+  cudaEvent_t a, b;
+  check_cuda(cudaEventCreate(&a), "event");
+  check_cuda(cudaEventCreate(&b), "event");
+  for (int st = 0; st < kStages; st++) {
+    check_cuda(cudaEventRecord(a, ctx->stream), "event record");
+    if (group == ZKG_G1) stage<Fq>(st, bases->ptr, scalars->ptr, ctx->stream);
+    else stage<Fq2>(st, bases->ptr, scalars->ptr, ctx->stream);
+    check_cuda(cudaEventRecord(b, ctx->stream), "event record");
+    check_cuda(cudaEventSynchronize(b), "msm stage");
+    float ms = 0;
+    check_cuda(cudaEventElapsedTime(&ms, a, b), "event time");
+    out.emplace_back(stage_name(st), (double)ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return out;
+}
+
+// ------------------------------------------------------------------ base upload
+
+// Rescales every coordinate in place on the device: v -> v * scale / 2^256.
+static void rescale(zkg_ctx* ctx, zkg_buf* buf, const host::U256& scale_mont) {
+  Fq s;
+  host::words32(scale_mont, s.w);
+  size_t coords = buf->words / 8;
+  if (coords == 0) return;
+  fq_rescale<<<grid_for(coords, 256), 256, 0, ctx->stream>>>(buf->ptr, coords, s);
+  check_launch("fq_rescale");
+}
+
+void upload_bases(zkg_ctx* ctx, const uint32_t* xy, size_t words, bool mont256, zkg_buf* out) {
+  (void)xy;
+  (void)words;
+  // Msm::upload_bases: scale = R^2 turns plain x into x*R (src/msm.rs:182-188).
+  // Msm::upload_bases_montgomery_256: the input is x*2^256 = x*R already (src/msm.rs:190-197).
+  if (!mont256) rescale(ctx, out, host::fq().r2);
+}
+
+}  // namespace zkg

@@ -1,0 +1,64 @@
+// MSM plan (host side of Msm, src/msm.rs:25-298).
+#pragma once
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "msm_common.hpp"
+#include "runtime.hpp"
+
+namespace zkg {
+
+uint32_t default_window(size_t n);
+void upload_bases(zkg_ctx* ctx, const uint32_t* xy, size_t words, bool mont256, zkg_buf* out);
+
+struct MsmPlan {
+  enum Stage {
+    kStageCount,
+    kStageScan,
+    kStageScatter,
+    kStageAccumulate,
+    kStageMerge,
+    kStageReduce,
+    kStageWindows,
+    kStageCombine,
+    kStages
+  };
+
+  zkg_ctx* ctx;
+  int group;
+  size_t n;
+  uint32_t c, windows = 0, half = 0, seg_len = 0;
+  size_t slots = 0, heads_max = 0;
+  uint32_t merge_levels = 0, scan_tiles_n = 0;
+  ReduceLevels levels;
+  std::vector<uint32_t> level_m;
+
+  DeviceArray counts, slot_start, cursor, tile_sums, sorted, buckets;
+  DeviceArray heads[2], head_keys[2];
+  DeviceArray tots, runs[2], window_sums, result;
+  zkg_buf result_handle;
+  StageTimer timer;
+
+  MsmPlan(zkg_ctx* ctx, int group, size_t n, uint32_t c, uint32_t item_points);
+  size_t xyzz_words() const;
+  size_t affine_words() const;
+  void check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const;
+  // Queues every stage on stream s (no host synchronisation).
+  void enqueue(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
+  void run(const zkg_buf* bases, const zkg_buf* scalars);
+  std::vector<std::pair<std::string, double>> profile(const zkg_buf* bases, const zkg_buf* scalars);
+  static const char* stage_name(int which);
+
+ private:
+  template <class F>
+  void stage(int which, const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
+};
+
+}  // namespace zkg
+
+struct zkg_msm {
+  zkg::MsmPlan plan;
+  template <class... A>
+  explicit zkg_msm(A&&... a) : plan(std::forward<A>(a)...) {}
+};

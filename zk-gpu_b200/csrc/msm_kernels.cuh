@@ -1,0 +1,443 @@
+// MSM device kernels (signed-digit Pippenger), templated on the coordinate field
+// (Fq for G1, Fq2 for G2).
+//
+// Pipeline for one run (reference stage in brackets):
+//   1. recode + count   per point, W signed c-bit digits; warp-aggregated histogram of
+//                       (window, |digit|) slots                    [msm_digits.wgsl, count]
+//   2. scan             exclusive prefix sum over all W*B slots -> slot_start, cursor
+//                                                                  [msm_scan.wgsl]
+//   3. recode + scatter point index (sign in bit 31) written to its slot's range, one u32 per
+//                       nonzero digit, warp-aggregated cursors     [msm_digits.wgsl, scatter]
+//   4. accumulate       the sorted array is cut into equal segments of L entries, one per
+//                       thread, regardless of bucket boundaries: every thread does exactly L
+//                       mixed additions, so skewed bucket sizes cannot unbalance the warps.
+//                       A bucket that starts in a segment is written by that segment's thread;
+//                       the parts of a bucket that continue into later segments ("heads")
+//                       are emitted per segment with the bucket's slot as key.
+//                                                                  [msm_accumulate.wgsl]
+//   5. merge levels     heads with equal keys are contiguous; each level sums runs of up to
+//                       L1 of them, adds runs that start in its range into the bucket, and
+//                       passes runs that continue from the previous range to the next level
+//                       (log_L1 levels)                            [msm_merge/finalize.wgsl]
+//   6. reduce levels    per window S_w = sum_b (b+1) * bucket_b, by chunked running sums:
+//                       chunk k of 16 buckets gives tot_k = sum_j (j+1) B_j and run_k =
+//                       sum_j B_j; S_w = sum_k tot_k + 16 * sum_k k * run_k, and the second
+//                       sum is the same problem over run_1.. (next level)
+//                                                                  [msm_reduce_chunks.wgsl,
+//                                                                   msm_sum.wgsl]
+//   7. window sums      per window, sum each level's tot_k and fold levels (x16 between)
+//   8. combine          Horner over windows, c doublings each      [msm_combine.wgsl]
+#pragma once
+#include "curve.cuh"
+#include "msm_common.hpp"
+
+namespace zkg {
+
+
+template <class F>
+struct PointWords {
+  static constexpr int affine = 2 * FieldWords<F>::value;
+  static constexpr int xyzz = 4 * FieldWords<F>::value;
+};
+
+// ------------------------------------------------------------------ recoding
+
+// Window w's raw c bits of the scalar (8 LE words). c <= 20 < 32, so two words suffice.
+__device__ __forceinline__ uint32_t window_bits(const uint32_t s[8], uint32_t pos, uint32_t c) {
+  uint32_t word = pos >> 5, off = pos & 31;
+  uint32_t v = 0;
+  if (word < 8) v = s[word] >> off;
+  if (off + c > 32 && word + 1 < 8) v |= s[word + 1] << (32 - off);
+  return v & ((1u << c) - 1);
+}
+
+__device__ __forceinline__ void load_scalar(const uint32_t* scalars, size_t i, uint32_t s[8]) {
+  const uint4* p = reinterpret_cast<const uint4*>(scalars + 8 * i);
+  uint4 lo = __ldg(p), hi = __ldg(p + 1);
+  s[0] = lo.x; s[1] = lo.y; s[2] = lo.z; s[3] = lo.w;
+  s[4] = hi.x; s[5] = hi.y; s[6] = hi.z; s[7] = hi.w;
+}
+
+// Digit recoding of msm_digits.wgsl:19-37: v = window + carry; v >= 2^(c-1) gives the
+// negative digit v - 2^c (magnitude 2^c - v) and a carry into the next window. Returns the
+// slot (w * B + |digit| - 1) or kNoKey for a zero digit; *neg gets the sign.
+struct Recoder {
+  uint32_t s[8];
+  uint32_t carry = 0;
+  __device__ __forceinline__ uint32_t next(uint32_t w, uint32_t c, uint32_t half, bool* neg) {
+    uint32_t v = window_bits(s, w * c, c) + carry;
+    carry = 0;
+    uint32_t mag = v;
+    *neg = false;
+    if (v >= half) {
+      mag = (1u << c) - v;
+      *neg = true;
+      carry = 1;
+    }
+    return mag ? w * half + mag - 1 : kNoKey;
+  }
+};
+
+// Pass 1: histogram of (window, bucket) slots. Lanes of a warp that hit the same slot are
+// merged into one atomic (equal scalars, zero-heavy or r-1-heavy inputs hammer single slots).
+__global__ void msm_count(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
+                          uint32_t* __restrict__ counts) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < n;
+  Recoder rc;
+  if (live) load_scalar(scalars, i, rc.s);
+  uint32_t half = 1u << (c - 1);
+  for (uint32_t w = 0; w < windows; w++) {
+    bool neg;
+    uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
+    unsigned active = __activemask();
+    unsigned peers = __match_any_sync(active, slot);
+    if (slot != kNoKey) {
+      int leader = __ffs(peers) - 1;
+      if ((int)(threadIdx.x & 31) == leader) atomicAdd(&counts[slot], (uint32_t)__popc(peers));
+    }
+  }
+}
+
+// Pass 3: scatter point indices (sign in bit 31) into slot order. Within a slot the order is
+// whatever the atomics give; bucket sums are exact, so the result does not depend on it.
+__global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
+                            uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < n;
+  Recoder rc;
+  if (live) load_scalar(scalars, i, rc.s);
+  uint32_t half = 1u << (c - 1);
+  unsigned lane = threadIdx.x & 31;
+  for (uint32_t w = 0; w < windows; w++) {
+    bool neg = false;
+    uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
+    unsigned active = __activemask();
+    unsigned peers = __match_any_sync(active, slot);
+    if (slot != kNoKey) {
+      int leader = __ffs(peers) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(&cursor[slot], (uint32_t)__popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      uint32_t rank = __popc(peers & ((1u << lane) - 1));
+      sorted[base + rank] = (uint32_t)i | (neg ? kNegBit : 0u);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ scan (3 phases)
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total, uint32_t* warp_sums) {
+  unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= (unsigned)d) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t s = lane < blockDim.x / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, s, d);
+      if (lane >= (unsigned)d) s += y;
+    }
+    warp_sums[lane] = s;  // inclusive
+  }
+  __syncthreads();
+  uint32_t before = warp ? warp_sums[warp - 1] : 0;
+  *total = warp_sums[blockDim.x / 32 - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const uint32_t* __restrict__ in, size_t len,
+                                                             uint32_t* __restrict__ tile_sums) {
+  __shared__ uint32_t warp_sums[32];
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++)
+    if (base + k < len) s += in[base + k];
+  uint32_t total;
+  block_exclusive_scan(s, &total, warp_sums);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Exclusive scan of the tile sums in place (tiles <= kScanTile), total into *grand.
+__global__ void __launch_bounds__(kScanBlock) scan_tiles(uint32_t* __restrict__ tile_sums, uint32_t tiles,
+                                                          uint32_t* __restrict__ grand) {
+  __shared__ uint32_t warp_sums[32];
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint32_t idx = threadIdx.x * kScanItems + k;
+    v[k] = idx < tiles ? tile_sums[idx] : 0;
+    s += v[k];
+  }
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(s, &total, warp_sums);
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint32_t idx = threadIdx.x * kScanItems + k;
+    if (idx < tiles) tile_sums[idx] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) *grand = total;
+}
+
+// out[i] = exclusive prefix of in; also copies it to out2 (the scatter cursor).
+__global__ void __launch_bounds__(kScanBlock) scan_apply(const uint32_t* __restrict__ in, size_t len,
+                                                         const uint32_t* __restrict__ tile_offsets,
+                                                         uint32_t* __restrict__ out, uint32_t* __restrict__ out2) {
+  __shared__ uint32_t warp_sums[32];
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    v[k] = base + k < len ? in[base + k] : 0;
+    s += v[k];
+  }
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(s, &total, warp_sums) + tile_offsets[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    if (base + k < len) {
+      out[base + k] = run;
+      out2[base + k] = run;
+    }
+    run += v[k];
+  }
+}
+
+// ------------------------------------------------------------------ accumulate
+
+// Largest s in [lo, hi) with a[s] <= p, given a[lo] <= p < a[hi].
+__device__ __forceinline__ uint32_t last_leq(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t p) {
+  while (hi - lo > 1) {
+    uint32_t mid = lo + (hi - lo) / 2;
+    if (__ldg(&a[mid]) <= p) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <class F>
+__device__ __forceinline__ Affine<F> load_signed_base(const uint32_t* __restrict__ bases, uint32_t entry) {
+  Affine<F> p = load_affine<F>(bases + (size_t)(entry & ~kNegBit) * PointWords<F>::affine);
+  if (entry & kNegBit) p.y = neg(p.y);
+  return p;
+}
+
+// One thread per segment [t*L, t*L + L) of the sorted entries (all windows concatenated, slot
+// order). slot_start has num_slots + 1 entries; slot_start[num_slots] = total entries.
+template <class F>
+__global__ void __launch_bounds__(128) msm_accumulate(const uint32_t* __restrict__ bases,
+                                                      const uint32_t* __restrict__ sorted,
+                                                      const uint32_t* __restrict__ slot_start, uint32_t num_slots,
+                                                      uint32_t seg_len, uint32_t* __restrict__ buckets,
+                                                      uint32_t* __restrict__ heads,
+                                                      uint32_t* __restrict__ head_keys) {
+  constexpr int XW = PointWords<F>::xyzz;
+  const uint32_t total = __ldg(&slot_start[num_slots]);
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t p0_64 = (uint64_t)t * seg_len;
+  if (p0_64 >= total) return;
+  const uint32_t p0 = (uint32_t)p0_64;
+  const uint64_t e64 = p0_64 + seg_len;
+  const uint32_t p1 = e64 < total ? (uint32_t)e64 : total;
+
+  uint32_t s = last_leq(slot_start, 0, num_slots, p0);
+  uint32_t end = __ldg(&slot_start[s + 1]);
+  bool head = __ldg(&slot_start[s]) < p0;  // the slot began in an earlier segment
+  uint32_t head_key = kNoKey;
+
+  Xyzz<F> acc = xyzz_infinity<F>();
+  uint32_t entry = __ldg(&sorted[p0]);
+  Affine<F> next = load_signed_base<F>(bases, entry);
+  for (uint32_t p = p0; p < p1; p++) {
+    Affine<F> cur = next;
+    if (p + 1 < p1) {
+      entry = __ldg(&sorted[p + 1]);
+      next = load_signed_base<F>(bases, entry);
+    }
+    if (p == end) {  // slot s is complete; move to the slot that holds position p
+      if (head) {
+        store_xyzz(heads + (size_t)t * XW, acc);
+        head_key = s;
+        head = false;
+      } else {
+        store_xyzz(buckets + (size_t)s * XW, acc);
+      }
+      acc = xyzz_infinity<F>();
+      uint32_t s2 = s + 1;
+      if (__ldg(&slot_start[s2 + 1]) <= p) s2 = last_leq(slot_start, s2, num_slots, p);
+      s = s2;
+      end = __ldg(&slot_start[s + 1]);
+    }
+    acc = xyzz_add_affine(acc, cur);
+  }
+  if (head) {
+    store_xyzz(heads + (size_t)t * XW, acc);
+    head_key = s;
+  } else {
+    store_xyzz(buckets + (size_t)s * XW, acc);
+  }
+  head_keys[t] = head_key;
+}
+
+// ------------------------------------------------------------------ merge levels
+
+// Length of the head array at merge level `level` (level 0 = the accumulate output).
+__device__ __forceinline__ uint32_t heads_len(uint32_t total, uint32_t seg_len, uint32_t level) {
+  uint64_t len = ((uint64_t)total + seg_len - 1) / seg_len;
+  for (uint32_t l = 0; l < level; l++) len = (len + kMergeFanIn - 1) / kMergeFanIn;
+  return (uint32_t)len;
+}
+
+template <class F>
+__device__ __forceinline__ void add_into_bucket(uint32_t* buckets, uint32_t key, const Xyzz<F>& v) {
+  constexpr int XW = PointWords<F>::xyzz;
+  uint32_t* b = buckets + (size_t)key * XW;
+  store_xyzz(b, xyzz_add(load_xyzz<F>(b), v));
+}
+
+// Thread u sums heads [u*L1, u*L1 + L1) of level `level`. Runs that start inside the range
+// are added into their bucket; a run that continues from the previous range becomes this
+// thread's head for the next level.
+template <class F>
+__global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ slot_start, uint32_t num_slots,
+                                                 uint32_t seg_len, uint32_t level,
+                                                 const uint32_t* __restrict__ in_pts,
+                                                 const uint32_t* __restrict__ in_keys, uint32_t* __restrict__ out_pts,
+                                                 uint32_t* __restrict__ out_keys, uint32_t* __restrict__ buckets) {
+  constexpr int XW = PointWords<F>::xyzz;
+  const uint32_t total = __ldg(&slot_start[num_slots]);
+  const uint32_t len = heads_len(total, seg_len, level);
+  if (len <= 1) return;  // nothing left to merge
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t q0_64 = (uint64_t)u * kMergeFanIn;
+  if (q0_64 >= len) return;
+  const uint32_t q0 = (uint32_t)q0_64, q1 = min(q0 + kMergeFanIn, len);
+  const uint32_t prev = q0 > 0 ? in_keys[q0 - 1] : kNoKey;
+
+  uint32_t cur = kNoKey, start = q0, out_key = kNoKey;
+  Xyzz<F> acc = xyzz_infinity<F>();
+  for (uint32_t q = q0; q <= q1; q++) {
+    uint32_t k = q < q1 ? in_keys[q] : kNoKey;
+    if (k != cur || q == q1) {
+      if (cur != kNoKey) {
+        if (start == q0 && prev == cur) {
+          store_xyzz(out_pts + (size_t)u * XW, acc);
+          out_key = cur;
+        } else {
+          add_into_bucket<F>(buckets, cur, acc);
+        }
+      }
+      if (q == q1) break;
+      cur = k;
+      start = q;
+      acc = xyzz_infinity<F>();
+    }
+    if (k != kNoKey) acc = xyzz_add(acc, load_xyzz<F>(in_pts + (size_t)q * XW));
+  }
+  out_keys[u] = out_key;
+}
+
+// ------------------------------------------------------------------ bucket reduction
+
+// Level of the running-sum reduction. Per window w the input holds m values A_0..A_{m-1} at
+// in + (w * in_stride + b) * XW; level 0 reads the buckets, where an empty slot (no entries)
+// is the point at infinity. Thread (w, k) covers b in [16k, 16k + 16):
+//   tot_k = sum_j (j+1) A_{16k+j}   -> tot_out[w * tot_stride + k]
+//   run_k = sum_j A_{16k+j}          -> run_out[w * run_stride + k - 1]  (k >= 1)
+template <class F>
+__global__ void __launch_bounds__(128) msm_reduce_level(const uint32_t* __restrict__ in, uint32_t in_stride,
+                                                        uint32_t m, uint32_t windows,
+                                                        const uint32_t* __restrict__ slot_start,
+                                                        uint32_t* __restrict__ tot_out, uint32_t tot_stride,
+                                                        uint32_t* __restrict__ run_out, uint32_t run_stride) {
+  constexpr int XW = PointWords<F>::xyzz;
+  const uint32_t chunks = (m + kChunk - 1) / kChunk;
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= chunks * windows) return;
+  const uint32_t w = id / chunks, k = id % chunks;
+  const uint32_t lo = k * kChunk, hi = min(lo + kChunk, m);
+  Xyzz<F> run = xyzz_infinity<F>(), tot = xyzz_infinity<F>();
+  for (uint32_t b = hi; b-- > lo;) {
+    size_t slot = (size_t)w * in_stride + b;
+    bool empty = slot_start && __ldg(&slot_start[slot]) == __ldg(&slot_start[slot + 1]);
+    if (!empty) run = xyzz_add(run, load_xyzz<F>(in + slot * XW));
+    tot = xyzz_add(tot, run);
+  }
+  store_xyzz(tot_out + ((size_t)w * tot_stride + k) * XW, tot);
+  if (k >= 1) store_xyzz(run_out + ((size_t)w * run_stride + k - 1) * XW, run);
+}
+
+
+// Block-wide sum of XYZZ values (one per thread) through shared memory.
+template <class F>
+__device__ Xyzz<F> block_sum(Xyzz<F> v, Xyzz<F>* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (unsigned stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) sh[threadIdx.x] = xyzz_add(sh[threadIdx.x], sh[threadIdx.x + stride]);
+    __syncthreads();
+  }
+  Xyzz<F> r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// One block per window: S_w = sum over levels l of 16^l * sum_k tot_l[k], folded from the top
+// level down (4 doublings per level).
+template <class F>
+__global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t* __restrict__ tots, ReduceLevels lv,
+                                                                  uint32_t* __restrict__ window_sums) {
+  constexpr int XW = PointWords<F>::xyzz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Xyzz<F>* sh = reinterpret_cast<Xyzz<F>*>(smem_raw);
+  const uint32_t w = blockIdx.x;
+  Xyzz<F> acc = xyzz_infinity<F>();
+  for (int l = (int)lv.count - 1; l >= 0; l--) {
+    Xyzz<F> part = xyzz_infinity<F>();
+    const uint32_t* base = tots + ((size_t)lv.tot_offset[l] + (size_t)w * lv.tot_len[l]) * XW;
+    for (uint32_t k = threadIdx.x; k < lv.tot_len[l]; k += blockDim.x) part = xyzz_add(part, load_xyzz<F>(base + (size_t)k * XW));
+    part = block_sum(part, sh);
+    if (threadIdx.x == 0) {
+      for (int d = 0; d < 4; d++) acc = xyzz_double(acc);  // x16 = kChunk
+      acc = xyzz_add(acc, part);
+    }
+  }
+  if (threadIdx.x == 0) store_xyzz(window_sums + (size_t)w * XW, acc);
+}
+
+// result = sum_w 2^(c*w) S_w by Horner from the top window (msm_combine.wgsl:13-22).
+template <class F>
+__global__ void msm_combine(const uint32_t* __restrict__ window_sums, uint32_t windows, uint32_t c,
+                            uint32_t* __restrict__ result) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  constexpr int XW = PointWords<F>::xyzz;
+  Xyzz<F> acc = load_xyzz<F>(window_sums + (size_t)(windows - 1) * XW);
+  for (int w = (int)windows - 2; w >= 0; w--) {
+    for (uint32_t k = 0; k < c; k++) acc = xyzz_double(acc);
+    acc = xyzz_add(acc, load_xyzz<F>(window_sums + (size_t)w * XW));
+  }
+  store_xyzz(result, acc);
+}
+
+// ------------------------------------------------------------------ base upload
+
+// x <- x * scale / 2^256 for every 8-word Fq coordinate (to_montgomery.wgsl:6-15). With
+// scale = 2^512 mod q this maps plain coordinates to Montgomery form; (0,0) stays (0,0).
+__global__ void fq_rescale(uint32_t* __restrict__ coords, size_t count, Fq scale) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  store_fe(coords + 8 * i, load_fe<Fq>(coords + 8 * i) * scale);
+}
+
+}  // namespace zkg

@@ -1,0 +1,196 @@
+// Fr NTT (src/ntt.rs:1-119, src/shaders/ntt.wgsl, src/shaders/twiddles.wgsl) on sm_100a.
+//
+// Decimation-in-frequency radix-2, natural order in and out, in place from the caller's view;
+// the inverse includes the 1/n factor. Data stays in plain form and twiddles carry the
+// Montgomery factor, so a Montgomery product x * tw returns exactly x * w^j (the reference's
+// convention, src/ntt.rs:3-5).
+//
+// The log_n stages run as passes over shared-memory tiles of 2^11 elements (64 KiB; three
+// tiles per SM): a pass of s stages loads 2^(11-s) consecutive columns of 2^s rows (rows are
+// 2^lm elements apart), so every global access is a run of at least four 32-byte elements.
+// The first pass reads the caller's buffer into the plan's scratch, middle passes work in
+// place on the scratch, and the last pass writes back in bit-reversed order (fused with the
+// 1/n scaling for the inverse). Transforms of at most 2^11 elements are one tile in one block.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "field.cuh"
+#include "host_field.hpp"
+#include "ntt.hpp"
+
+namespace zkg {
+
+constexpr uint32_t kTileLog = 11;
+constexpr uint32_t kNttThreads = 256;
+constexpr uint32_t kMaxStagesPerPass = 9;
+
+// tw[j] = hi[j >> lo_bits] * lo[j & (2^lo_bits - 1)], j < count (twiddles.wgsl:13-21).
+__global__ void ntt_twiddles(const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint32_t lo_bits,
+                             size_t count, uint32_t* __restrict__ out) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  Fr a = load_fe<Fr>(hi + 8 * (j >> lo_bits));
+  Fr b = load_fe<Fr>(lo + 8 * (j & ((1ull << lo_bits) - 1)));
+  store_fe(out + 8 * j, a * b);
+}
+
+__device__ __forceinline__ uint32_t tile_global_index(uint32_t tile, uint32_t slot, uint32_t lg, uint32_t lm,
+                                                      uint32_t s) {
+  uint32_t row = slot >> lg;
+  uint32_t col = slot & ((1u << lg) - 1);
+  uint32_t c = (tile << lg) + col;  // column id over the whole array
+  uint32_t j0 = c & ((1u << lm) - 1);
+  return ((c >> lm) << (lm + s)) + j0 + (row << lm);
+}
+
+// One pass: stages [log_n - lm - s, log_n - lm) on tiles of 2^tl elements.
+template <bool LAST>
+__global__ void __launch_bounds__(kNttThreads, 3)
+    ntt_pass(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const uint32_t* __restrict__ tw,
+             uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale) {
+  extern __shared__ __align__(16) uint32_t tile_words[];
+  const uint32_t lg = tl - s;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t elems = 1u << tl;
+
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    store_fe(tile_words + 8 * slot, load_fe_cg<Fr>(src + 8 * (size_t)g));
+  }
+  __syncthreads();
+
+  const uint32_t t0 = log_n - lm - s;  // global index of the pass's first stage
+  const uint32_t half_elems = elems >> 1;
+  for (uint32_t st = 0; st < s; st++) {
+    const uint32_t lh = s - 1 - st;  // log2 of the row distance
+    const uint32_t t = t0 + st;      // global stage
+    for (uint32_t b = threadIdx.x; b < half_elems; b += kNttThreads) {
+      uint32_t col = b & ((1u << lg) - 1);
+      uint32_t q = b >> lg;
+      uint32_t r_lo = q & ((1u << lh) - 1);
+      uint32_t row_a = ((q >> lh) << (lh + 1)) + r_lo;
+      uint32_t slot_a = (row_a << lg) + col;
+      uint32_t slot_b = slot_a + (1u << (lh + lg));
+      uint32_t c = (tile << lg) + col;
+      uint32_t j0 = c & ((1u << lm) - 1);
+      uint32_t idx = ((r_lo << lm) + j0) << t;
+      Fr x = load_fe<Fr>(tile_words + 8 * slot_a);
+      Fr y = load_fe<Fr>(tile_words + 8 * slot_b);
+      Fr d = x - y;
+      store_fe(tile_words + 8 * slot_a, x + y);
+      if (idx != 0) d = d * load_fe<Fr>(tw + 8 * (size_t)idx);
+      store_fe(tile_words + 8 * slot_b, d);
+    }
+    __syncthreads();
+  }
+
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    Fr v = load_fe<Fr>(tile_words + 8 * slot);
+    if (scale_flag) v = v * scale;
+    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    if (LAST) g = __brev(g) >> (32 - log_n);
+    store_fe(dst + 8 * (size_t)g, v);
+  }
+}
+
+static std::vector<uint32_t> powers_words(const host::U256& step, size_t len) {
+  const host::Field& f = host::fr();
+  std::vector<uint32_t> out(8 * len);
+  host::U256 x = f.one;  // Montgomery 1
+  for (size_t i = 0; i < len; i++) {
+    host::words32(x, &out[8 * i]);
+    x = host::mul(x, step, f);
+  }
+  return out;
+}
+
+NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
+  if (log_n < 10 || log_n > 27) fail(ZKG_EINVAL, "log_n must be in 10..=27");
+  use(ctx);
+  const host::Field& f = host::fr();
+  const size_t n = (size_t)1 << log_n;
+  host::U256 w = host::root_of_unity(log_n);  // Montgomery form
+  host::U256 w_inv = host::inverse(w, f);
+  // n^-1 * R (src/ntt.rs:32): Montgomery form of 1/n
+  host::U256 n_inv = host::inverse(host::to_mont(host::U256{{(uint64_t)n, 0, 0, 0}}, f), f);
+  host::words32(n_inv, n_inv_words);
+
+  scratch.alloc(8 * n, "ntt scratch");
+  build_twiddles(w, fwd_tw);
+  build_twiddles(w_inv, inv_tw);
+
+  // Pass split: one tile when it fits, else ceil(log_n / 9) passes of near-equal size.
+  if (log_n <= kTileLog) {
+    passes.push_back(log_n);
+  } else {
+    uint32_t p = (log_n + kMaxStagesPerPass - 1) / kMaxStagesPerPass;
+    for (uint32_t i = 0; i < p; i++) passes.push_back(log_n / p + (i < log_n % p ? 1u : 0u));
+  }
+  const size_t smem = (size_t)32 << (log_n < kTileLog ? log_n : kTileLog);
+  check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "ntt smem attribute");
+}
+
+void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out) {
+  const host::Field& f = host::fr();
+  const size_t count = (size_t)1 << (log_n - 1);
+  const uint32_t lo_bits = (log_n - 1 + 1) / 2;  // ceil((log_n - 1) / 2)
+  const size_t lo_len = (size_t)1 << lo_bits;
+  const size_t hi_len = (count + lo_len - 1) / lo_len;
+  std::vector<uint32_t> lo = powers_words(root, lo_len);
+  host::U256 step = host::pow(root, host::U256{{(uint64_t)lo_len, 0, 0, 0}}, f);
+  std::vector<uint32_t> hi = powers_words(step, hi_len);
+  DeviceArray dlo, dhi;
+  dlo.alloc(lo.size(), "ntt twiddle seeds");
+  dhi.alloc(hi.size(), "ntt twiddle seeds");
+  check_cuda(cudaMemcpyAsync(dlo.ptr, lo.data(), lo.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "twiddle copy");
+  check_cuda(cudaMemcpyAsync(dhi.ptr, hi.data(), hi.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "twiddle copy");
+  out.alloc(8 * count, "ntt twiddles");
+  ntt_twiddles<<<grid_for(count, 256), 256, 0, ctx->stream>>>(dhi.ptr, dlo.ptr, lo_bits, count, out.ptr);
+  check_launch("ntt_twiddles");
+  // The seed arrays are freed when this function returns: wait for the kernel first.
+  check_cuda(cudaStreamSynchronize(ctx->stream), "ntt twiddles");
+}
+
+void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
+  const uint32_t* tw = inverse ? inv_tw.ptr : fwd_tw.ptr;
+  Fr scale;
+  std::memcpy(scale.w, n_inv_words, sizeof(scale.w));
+  const uint32_t tl = log_n < kTileLog ? log_n : kTileLog;
+  const unsigned tiles = 1u << (log_n - tl);
+  const size_t smem = (size_t)32 << tl;
+  uint32_t done = 0;
+  const size_t np = passes.size();
+  for (size_t i = 0; i < np; i++) {
+    const uint32_t st = passes[i];
+    const uint32_t lm = log_n - done - st;
+    const bool last = i + 1 == np;
+    const uint32_t* src = i == 0 ? data : scratch.ptr;
+    uint32_t* dst = last ? data : scratch.ptr;
+    const int scale_flag = last && inverse;
+    size_t ev = timer.enabled ? timer.begin((int)i, s) : 0;
+    if (last)
+      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+    else
+      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+    check_launch("ntt_pass");
+    if (timer.enabled) timer.end(ev, s);
+    done += st;
+  }
+  if (timer.enabled) timer.runs++;
+}
+
+void NttPlan::run(zkg_buf* data, bool inverse) {
+  const size_t need = (size_t)32 << log_n;
+  const size_t have = data->words * 4;
+  if (have < need)
+    fail(ZKG_ESIZE, "data buffer holds " + std::to_string(have) + " bytes; a 2^" + std::to_string(log_n) +
+                        " transform needs " + std::to_string(need));
+  use(ctx);
+  enqueue(data->ptr, inverse, ctx->stream);
+}
+
+}  // namespace zkg

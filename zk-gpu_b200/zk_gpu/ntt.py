@@ -1,0 +1,49 @@
+"""ntt::Ntt (src/ntt.rs:14-50) over zkg_ntt."""
+from __future__ import annotations
+
+import ctypes
+
+from ._lib import check, lib, vp
+from .gpu import Buffer, Gpu
+
+
+class Ntt:
+    """Plan for in-place transforms of 2^log_n Fr elements (10 <= log_n <= 27), natural order
+    in and out; buffers hold 8 plain u32 words per element."""
+
+    def __init__(self, gpu: Gpu, log_n: int):
+        h = vp()
+        check(lib().zkg_ntt_new(gpu.handle, log_n, ctypes.byref(h)))
+        self._h = h.value
+        self._gpu = gpu
+
+    @classmethod
+    def new(cls, gpu: Gpu, log_n: int) -> "Ntt":
+        return cls(gpu, log_n)
+
+    @property
+    def log_n(self) -> int:
+        return lib().zkg_ntt_log_n(self._h)
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def forward(self, gpu: Gpu, data: Buffer) -> None:
+        """In-place forward transform (Radix2EvaluationDomain::fft)."""
+        check(lib().zkg_ntt_forward(self._h, data.handle))
+
+    def inverse(self, gpu: Gpu, data: Buffer) -> None:
+        """In-place inverse transform, including the 1/n factor."""
+        check(lib().zkg_ntt_inverse(self._h, data.handle))
+
+    def close(self) -> None:
+        if self._h:
+            lib().zkg_ntt_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
