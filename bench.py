@@ -1,0 +1,463 @@
+#!/usr/bin/env python
+"""Benchmark: BN254 MSM and Fr NTT on B200, through the library's C ABI.
+
+One step is the workload the headline metric names, with inputs resident in HBM:
+    G1 MSM n = 2^24 + G1 MSM n = 2^20 (default_window, uniform scalars in [0, r),
+    bases [k_i]G1 for seeded uniform k_i with 0.1% at infinity, kept in Montgomery form)
+    + Fr NTT 2^24 forward then inverse (in place, natural order).
+`value` is milliseconds per step (device time, CUDA events on the library's stream, max over
+ranks); `e2e` is the same step through the public API with pinned host buffers: scalars and NTT
+input copied host->device, MSM results and NTT outputs read back, every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU path: the C restatement of zk-gpu's MSM and NTT
+(oracle/, multi-threaded over every host core; the reference itself is Rust + wgpu and
+cannot be built or run here) on the same step. Multi-GPU runs are independent replicas (the
+MSM and NTT of one proof do not shard across GPUs here), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "zk-gpu_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "MSM 2^20/2^24 & NTT 2^24 ms, bit-exact; batched vs plain req/s, p50/p99 ms"
+IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m), field.cuh
+MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
+# ncu DRAM traffic (read + write bytes) per launch, from profiles/*.md (see the file named
+# in each entry); None until captured.
+NCU_TRAFFIC = {
+    "msm_accumulate_2^24": None,
+    "ntt_pass_2^24": None,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log-msm", type=int, default=24, help="large MSM size (log2); 24 in the benchmark")
+    ap.add_argument("--log-msm-small", type=int, default=20)
+    ap.add_argument("--log-ntt", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a) -> str:
+    return (f"BN254 G1 MSM n=2^{a.log_msm} + G1 MSM n=2^{a.log_msm_small} (default_window, uniform scalars in [0,r), "
+            f"bases [k_i]G1 with 0.1% at infinity, resident in Montgomery form) + Fr NTT 2^{a.log_ntt} forward "
+            f"then inverse (in place, natural order)")
+
+
+# ---------------------------------------------------------------- distributed plumbing
+
+class Dist:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        self.target = ids[local_rank] if local_rank < len(ids) else str(local_rank)
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{local_rank}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", self.target, "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons = [], [], set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(self.NAMES, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(a, d: Dist) -> dict | None:
+    import torch
+
+    from zk_gpu import Gpu, Group, Msm, Ntt, lib, xyzz_to_affine
+    from zk_gpu._lib import StageTime, check
+    from zk_gpu.msm import affine_words
+    from zk_gpu.synthetic import generator_multiples, infinity_mask, uniform_scalars
+
+    L = lib()
+    torch.cuda.set_device(d.local_rank)
+    gpu = Gpu(d.local_rank)
+    stream = torch.cuda.ExternalStream(L.zkg_ctx_stream(gpu.handle), device=torch.device("cuda", d.local_rank))
+    n24, n20, nn = 1 << a.log_msm, 1 << a.log_msm_small, 1 << a.log_ntt
+
+    # inputs (seeded; identical on every rank: weak scaling, one replica per GPU)
+    k = uniform_scalars(n24, 101).reshape(n24, 8)
+    k[infinity_mask(n24, 0.001, 102)] = 0
+    k = k.reshape(-1)
+    bases = generator_multiples(gpu, Group.G1, k, mont256=True)  # resident proving key
+    s24_host = uniform_scalars(n24, 103)
+    s20_host = uniform_scalars(n20, 104)
+    x_host = uniform_scalars(nn, 105)
+    s24, s20, data = gpu.buffer(s24_host), gpu.buffer(s20_host), gpu.buffer(x_host)
+    c24, c20 = Msm.default_window(n24), Msm.default_window(n20)
+    msm24, msm20, ntt = Msm(gpu, n24, c24), Msm(gpu, n20, c20), Ntt(gpu, a.log_ntt)
+
+    def step():
+        msm24.run(gpu, bases, s24)
+        msm20.run(gpu, bases, s20)  # the first 2^20 points of the same key
+        ntt.forward(gpu, data)
+        ntt.inverse(gpu, data)
+
+    for _ in range(a.warmup):
+        step()
+    gpu.wait()
+    res24 = affine_words(xyzz_to_affine(gpu.read(msm24.run(gpu, bases, s24), 32)))
+    res20 = affine_words(xyzz_to_affine(gpu.read(msm20.run(gpu, bases, s20), 32)))
+    round_trip = bool(np.array_equal(gpu.read(data, x_host.size), x_host))
+    fwd_probe = gpu.buffer(x_host)
+    ntt.forward(gpu, fwd_probe)
+    ntt_fwd = gpu.read(fwd_probe, 8 * 4)  # first four outputs, checked against the CPU below
+    del fwd_probe
+    entries = ctypes.c_uint64()
+    check(L.zkg_msm_last_entries(msm24.__dict__["_h"], ctypes.byref(entries)))
+
+    # ---- timed region: device time of K steps
+    for h in (msm24._h, msm20._h):
+        check(L.zkg_msm_set_timing(h, 1))
+    check(L.zkg_ntt_set_timing(ntt.handle, 1))
+    clocks = ClockSampler(d.local_rank)
+    clocks.start()
+    time.sleep(0.4)
+    d.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.zkg_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    d.barrier()
+    launches = L.zkg_launch_count() - launches0
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    ms_step = d.max(ms_total / a.steps)
+
+    def stage_times(fn, h, cap=16):
+        arr = (StageTime * cap)()
+        cnt, runs = ctypes.c_size_t(), ctypes.c_size_t()
+        check(fn(h, arr, cap, ctypes.byref(cnt), ctypes.byref(runs)))
+        return {arr[i].stage.decode(): arr[i].ms / max(runs.value, 1) for i in range(cnt.value)}, runs.value
+
+    st24, _ = stage_times(L.zkg_msm_stage_times, msm24._h)
+    st20, _ = stage_times(L.zkg_msm_stage_times, msm20._h)
+    stn, nruns = stage_times(L.zkg_ntt_pass_times, ntt.handle)
+    for h in (msm24._h, msm20._h):
+        check(L.zkg_msm_set_timing(h, 0))
+    check(L.zkg_ntt_set_timing(ntt.handle, 0))
+
+    # ---- integer-multiply pipe peak (measured here, the roofline denominator for the MSM)
+    peaks = {}
+    for v, name in enumerate(["mad_lo", "mad_hi", "madc_chain", "fq_mulmod"]):
+        x = ctypes.c_double()
+        check(L.zkg_bench_integer_pipe(gpu.handle, v, ctypes.byref(x)))
+        peaks[name] = x.value
+    imad_peak = max(peaks["mad_lo"], peaks["mad_hi"], peaks["madc_chain"])
+
+    # ---- end to end through the public API with pinned host buffers
+    def pinned(words: int) -> np.ndarray:
+        ptr = ctypes.c_void_p()
+        check(L.zkg_host_alloc(words * 4, ctypes.byref(ptr)))
+        arr = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint32)), shape=(words,))
+        pinned.ptrs.append(ptr)
+        return arr
+    pinned.ptrs = []
+    p24, p20, px, pout = pinned(s24_host.size), pinned(s20_host.size), pinned(x_host.size), pinned(x_host.size)
+    p24[:], p20[:], px[:] = s24_host, s20_host, x_host
+    from zk_gpu._lib import u32p
+
+    def e2e_step():
+        s24.write(p24)
+        r = msm24.run(gpu, bases, s24)
+        gpu.read(r, 32)
+        s20.write(p20)
+        r = msm20.run(gpu, bases, s20)
+        gpu.read(r, 32)
+        data.write(px)
+        ntt.forward(gpu, data)
+        check(L.zkg_buf_read(gpu.handle, data.handle, pout.ctypes.data_as(u32p), pout.size))
+        ntt.inverse(gpu, data)
+        check(L.zkg_buf_read(gpu.handle, data.handle, pout.ctypes.data_as(u32p), pout.size))
+
+    e2e_step()
+    d.barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        e2e_step()
+    e2e_ms = d.max((time.perf_counter() - t0) * 1e3 / a.steps)
+    e2e_ok = bool(np.array_equal(pout, x_host))
+    for ptr in pinned.ptrs:
+        L.zkg_host_free(ptr)
+
+    # ---- rooflines
+    acc_ms = st24.get("accumulate", float("nan"))
+    acc_ops = entries.value * MULMODS_PER_MADD * IMAD_PER_MULMOD
+    acc_achieved = acc_ops / (acc_ms * 1e-3)
+    n_pass = len(stn)
+    ntt_pass_ms = sum(stn.values()) / max(n_pass, 1)  # mean pass duration (forward and inverse)
+    ntt_bytes = 64 * nn  # each pass reads and writes 32 B per element
+    hbm_peak = None
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        hbm_src = "measured"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback"
+    ntt_gbs = ntt_bytes / (ntt_pass_ms * 1e-3) / 1e9
+
+    out = {
+        "metric": METRIC,
+        "value": round(ms_step, 4),
+        "unit": "ms",
+        "n_gpus": d.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": round(ms_step, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32 (BN254 Fq/Fr Montgomery, 8x32-bit limbs)",
+        "data": "synthetic (seeded)",
+        "config": {
+            "workload": workload_name(a),
+            "parallelism": f"replicas x{d.world} (one full step per GPU)",
+            "windows": {"msm_2^%d" % a.log_msm: c24, "msm_2^%d" % a.log_msm_small: c20},
+            "l2": "inputs larger than L2 (2^24 MSM bases 1 GiB, scalars 512 MiB; NTT 512 MiB); no flush",
+        },
+        "parts_ms": {
+            f"msm_g1_2^{a.log_msm}": round(sum(st24.values()), 4),
+            f"msm_g1_2^{a.log_msm_small}": round(sum(st20.values()), 4),
+            f"ntt_2^{a.log_ntt}_per_transform": round(sum(stn.values()), 4),
+        },
+        "stages_ms": {f"msm_2^{a.log_msm}": {k: round(v, 4) for k, v in st24.items()},
+                      f"msm_2^{a.log_msm_small}": {k: round(v, 4) for k, v in st20.items()},
+                      f"ntt_2^{a.log_ntt}": {k: round(v, 4) for k, v in stn.items()}},
+        "roofline": {
+            "kernel": f"msm_accumulate<Fq> (G1 MSM 2^{a.log_msm})",
+            "bound": "imad",
+            "achieved": round(acc_achieved / 1e12, 3),
+            "peak": round(imad_peak / 1e12, 3),
+            "unit": "T int-mul-add/s",
+            "frac": round(acc_achieved / imad_peak, 4),
+            "traffic": NCU_TRAFFIC["msm_accumulate_2^24"],
+            "algorithmic": f"{entries.value} nonzero digits x {MULMODS_PER_MADD} Fq products x "
+                           f"{IMAD_PER_MULMOD} multiply-adds",
+            "peak_source": "measured in this run: best of mad.lo / mad.hi / carry-chain probes "
+                           "(zkg_bench_integer_pipe)",
+        },
+        "roofline_ntt": {
+            "kernel": f"ntt_pass (Fr NTT 2^{a.log_ntt}, {n_pass} passes)",
+            "bound": "hbm",
+            "achieved": round(ntt_gbs, 1),
+            "peak": hbm_peak,
+            "unit": "GB/s",
+            "frac": round(ntt_gbs / hbm_peak, 4),
+            "peak_source": hbm_src,
+            "traffic": NCU_TRAFFIC["ntt_pass_2^24"],
+            "algorithmic": "64 B per element per pass (read + write)",
+            "transform_frac_of_hbm": round((ntt_bytes * n_pass / (sum(stn.values()) * 1e-3) / 1e9) / hbm_peak, 4),
+        },
+        "integer_pipe_probe": {k: round(v / 1e12, 3) for k, v in peaks.items()},
+        "e2e": {
+            "value": round(e2e_ms, 3),
+            "unit": "ms",
+            "h2d_bytes_per_step": int(4 * (s24_host.size + s20_host.size + x_host.size)),
+            "d2h_bytes_per_step": int(4 * (32 + 32 + 2 * x_host.size)),
+        },
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "bit_exact": {"ntt_round_trip": round_trip, "e2e_round_trip": e2e_ok},
+    }
+    if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
+        out["cpu_baseline"], checks = cpu_baseline(a, gpu, bases, k, s20_host, s24_host, x_host, res20, res24,
+                                                   ntt_fwd)
+        out["bit_exact"].update(checks)
+    del msm24, msm20, ntt
+    return out
+
+
+# ---------------------------------------------------------------- CPU side (the oracle: baseline only)
+
+def cpu_step(bases_m256, s24, s20, x, threads):
+    """One step of the workload on the host cores with the C restatement of the reference's CPU
+    path. Returns (seconds per part, results)."""
+    from oracle import cpu
+
+    t = {}
+    t0 = time.perf_counter()
+    r24 = cpu.msm("G1", bases_m256, s24, mont256=True, nthreads=threads)
+    t["msm_2^24"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r20 = cpu.msm("G1", bases_m256[: s20.size * 2], s20, mont256=True, nthreads=threads)
+    t["msm_2^20"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    y = cpu.ntt(x, False, threads)
+    t["ntt_fwd"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cpu.ntt(y, True, threads)
+    t["ntt_inv"] = time.perf_counter() - t0
+    return t, (r24, r20, y)
+
+
+def cpu_baseline(a, gpu, bases, k, s20, s24, x, res20, res24, ntt_fwd):
+    from oracle import cpu
+
+    threads = os.cpu_count() or 1
+    bases_m256 = gpu.read(bases, 16 * (1 << a.log_msm))
+    t, (r24, r20, y) = cpu_step(bases_m256, s24, s20, x, threads)
+    total = sum(t.values())
+    checks = {
+        f"msm_2^{a.log_msm}_vs_cpu": bool(np.array_equal(r24, res24)),
+        f"msm_2^{a.log_msm_small}_vs_cpu": bool(np.array_equal(r20, res20)),
+        f"ntt_2^{a.log_ntt}_vs_cpu": bool(np.array_equal(y[:32], ntt_fwd)),
+    }
+    return {"value": round(total * 1e3, 1), "unit": "ms", "cores": threads, "kind": "port",
+            "sample": "one full step (both MSMs and the NTT pair) on the oracle's C restatement of the "
+                      "reference's CPU algorithms", "parts_s": {k_: round(v, 3) for k_, v in t.items()}}, checks
+
+
+def run_reference(a, d: Dist) -> dict | None:
+    if d.rank != 0:
+        return None
+    from oracle import cpu
+    from zk_gpu.synthetic import infinity_mask, uniform_scalars
+
+    threads = os.cpu_count() or 1
+    n24, n20, nn = 1 << a.log_msm, 1 << a.log_msm_small, 1 << a.log_ntt
+    k = uniform_scalars(n24, 101).reshape(n24, 8)
+    k[infinity_mask(n24, 0.001, 102)] = 0
+    bases = cpu.generator_multiples("G1", k.reshape(-1), mont256=True, nthreads=threads)
+    s24, s20, x = uniform_scalars(n24, 103), uniform_scalars(n20, 104), uniform_scalars(nn, 105)
+    for _ in range(a.warmup):
+        cpu_step(bases, s24, s20, x, threads)
+    t0 = time.perf_counter()
+    parts = []
+    for _ in range(a.steps):
+        t, _ = cpu_step(bases, s24, s20, x, threads)
+        parts.append(t)
+    ms = (time.perf_counter() - t0) * 1e3 / a.steps
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(ms, 1),
+        "unit": "ms",
+        "n_gpus": d.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": round(ms, 1),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64 (BN254 Fq/Fr Montgomery, 4x64-bit limbs)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": workload_name(a), "parallelism": "host cores (rank 0 only)"},
+        "cpu_baseline": {"value": round(ms, 1), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": "the full step, every step (C restatement of the reference's CPU algorithms; "
+                                   "arkworks is not available here)"},
+        "e2e": {"value": round(ms, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "parts_s": {key: round(statistics.mean(p[key] for p in parts), 3) for key in parts[0]},
+    }
+
+
+def main():
+    a = parse()
+    d = Dist(a.gpus)
+    try:
+        out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)
+        if d.rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

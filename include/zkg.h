@@ -153,6 +153,9 @@ void zkg_host_free(void *p);
  * *runs receives the number of runs summed. */
 int zkg_msm_set_timing(zkg_msm *msm, int enable);
 int zkg_msm_stage_times(zkg_msm *msm, zkg_stage_time *out, size_t cap, size_t *count, size_t *runs);
+/* Number of (point, window) entries with a nonzero digit in the last run (blocking): the
+ * mixed additions the accumulation performed, for throughput accounting. */
+int zkg_msm_last_entries(zkg_msm *msm, uint64_t *entries);
 /* The same for the NTT: one entry per pass ("pass 0", "pass 1", ...), forward and inverse
  * transforms summed together. */
 int zkg_ntt_set_timing(zkg_ntt *ntt, int enable);
@@ -163,7 +166,7 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
 /* Throughput probe of the integer multiply-add pipe (the reference's examples/field_bench.rs
  * measures mulmods per second the same way): variant 0 = mad.lo.u32, 1 = mad.hi.u32,
  * 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq Montgomery
- * products. *ops_per_second receives multiply-adds (or products) per second on the context's
+ * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds). *ops_per_second receives multiply-adds (or products) per second on the context's
  * device; the best of five launches over every SM. */
 int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
 

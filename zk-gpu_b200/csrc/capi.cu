@@ -393,6 +393,20 @@ int zkg_msm_stage_times(zkg_msm* msm, zkg_stage_time* out, size_t cap, size_t* c
   });
 }
 
+int zkg_msm_last_entries(zkg_msm* msm, uint64_t* entries) {
+  return guard([&] {
+    need(msm, "msm");
+    need(entries, "entries");
+    use(msm->plan.ctx);
+    uint32_t v = 0;
+    check_cuda(cudaMemcpyAsync(&v, msm->plan.slot_start.ptr + msm->plan.slots, 4, cudaMemcpyDeviceToHost,
+                               msm->plan.ctx->stream),
+               "entry count");
+    check_cuda(cudaStreamSynchronize(msm->plan.ctx->stream), "entry count");
+    *entries = v;
+  });
+}
+
 int zkg_ntt_set_timing(zkg_ntt* ntt, int enable) {
   return guard([&] {
     need(ntt, "ntt");
@@ -416,7 +430,7 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 3) fail(ZKG_EINVAL, "variant must be 0..3");
+    if (variant < 0 || variant > 5) fail(ZKG_EINVAL, "variant must be 0..5");
     *ops_per_second = bench_integer_pipe(ctx, variant);
   });
 }

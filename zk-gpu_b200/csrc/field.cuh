@@ -1,6 +1,7 @@
 // BN254 base field Fq and scalar field Fr on sm_100a: 8 x 32-bit limbs, Montgomery radix
-// R = 2^256, products on the integer multiply-add pipe through PTX carry chains
-// (mad.lo.cc / madc.hi.cc). No tensor cores: this is exact modular integer arithmetic.
+// R = 2^256, products on the integer multiply-add pipe (mad.wide.u32) with PTX carry chains
+// (add.cc / addc) for the accumulation. No tensor cores: this is exact modular integer
+// arithmetic.
 //
 // Replaces the reference's generated WGSL field code (src/field.rs:55-181: 20 x 13-bit limbs,
 // R = 2^260, deferred carries). Memory format is unchanged: 8 little-endian u32 words per
@@ -145,70 +146,73 @@ __device__ __forceinline__ Fp<P> dbl(const Fp<P>& a) {
 }
 
 // ------------------------------------------------------------------ Montgomery product
+//
+// Coarsely integrated operand scanning with 32x32 -> 64-bit products. On sm_100a the wide
+// multiply (mad.wide.u32, one instruction for both halves of a product plus a 32-bit addend)
+// issues at the same rate as mul.hi alone, so a row x*v costs 8 wide multiply-adds on the
+// integer multiply pipe and one 8-long add.cc chain on the integer add pipe, instead of 8 low
+// plus 8 high multiply-adds: 2/3 of the multiply-pipe time of the lo/hi formulation, and the 8
+// products of a row are independent (a short dependency chain for single-thread latency).
+//
+// Row i (product or reduction) with d_j = x * v_j + t[i+j] < 2^64:
+//   t[i] = lo(d_0),  t[i+j] = lo(d_j) + hi(d_{j-1}) + carry (j = 1..7),
+//   t[i+8] (+)= hi(d_7) + carry.
+// The running value stays below 2^288 because p < 2^254, so word i+8 never carries out.
 
-// t[i..i+8] += a * bi. t[i+8] is fresh (never written before this row) and is set from the
-// carry of the low-half chain. Low halves land on t[i..i+7], high halves on t[i+1..i+8].
-#define ZKG_MAD_ROW(t, i, a, bi)                                                                  \
-  asm("mad.lo.cc.u32  %0, %9, %17, %0;\n\t"                                                        \
-      "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                       \
-      "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                       \
-      "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                       \
-      "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                       \
-      "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                       \
-      "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                       \
-      "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                       \
-      "addc.u32       %8, 0, 0;\n\t"                                                               \
-      "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"                                                        \
-      "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                       \
-      "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                       \
-      "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                       \
-      "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                       \
-      "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                       \
-      "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                       \
-      "madc.hi.u32    %8, %16, %17, %8;"                                                           \
-      : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]), "+r"(t[i + 5]), \
-        "+r"(t[i + 6]), "+r"(t[i + 7]), "=&r"(t[i + 8])                                              \
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(bi))
+// Product row: t[i+8] is fresh (never written before this row).
+#define ZKG_WIDE_CHAIN_FRESH(t, i, d)                                                            \
+  asm("add.cc.u32  %0, %8, %9;\n\t"                                                              \
+      "addc.cc.u32 %1, %10, %11;\n\t"                                                            \
+      "addc.cc.u32 %2, %12, %13;\n\t"                                                            \
+      "addc.cc.u32 %3, %14, %15;\n\t"                                                            \
+      "addc.cc.u32 %4, %16, %17;\n\t"                                                            \
+      "addc.cc.u32 %5, %18, %19;\n\t"                                                            \
+      "addc.cc.u32 %6, %20, %21;\n\t"                                                            \
+      "addc.u32    %7, %22, 0;"                                                                   \
+      : "=&r"(t[i + 1]), "=&r"(t[i + 2]), "=&r"(t[i + 3]), "=&r"(t[i + 4]), "=&r"(t[i + 5]),      \
+        "=&r"(t[i + 6]), "=&r"(t[i + 7]), "=&r"(t[i + 8])                                         \
+      : "r"((uint32_t)d[1]), "r"((uint32_t)(d[0] >> 32)), "r"((uint32_t)d[2]),                    \
+        "r"((uint32_t)(d[1] >> 32)), "r"((uint32_t)d[3]), "r"((uint32_t)(d[2] >> 32)),            \
+        "r"((uint32_t)d[4]), "r"((uint32_t)(d[3] >> 32)), "r"((uint32_t)d[5]),                    \
+        "r"((uint32_t)(d[4] >> 32)), "r"((uint32_t)d[6]), "r"((uint32_t)(d[5] >> 32)),            \
+        "r"((uint32_t)d[7]), "r"((uint32_t)(d[6] >> 32)), "r"((uint32_t)(d[7] >> 32)))
 
-// t[i..i+8] += m * p with m = t[i] * INV, which clears t[i]. The value stays below 2^288
-// because p < 2^254 (no carry out of t[i+8]).
-#define ZKG_RED_ROW(P, t, i)                                                                       \
-  do {                                                                                             \
-    uint32_t m_ = t[i] * P::INV;                                                                   \
-    asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                                      \
-        "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                                      \
-        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                      \
-        "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                                      \
-        "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                                      \
-        "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                                      \
-        "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                                      \
-        "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                                      \
-        "addc.u32       %8, %8, 0;\n\t"                                                            \
-        "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                                      \
-        "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                                      \
-        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                      \
-        "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                                      \
-        "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                                      \
-        "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                                      \
-        "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                                      \
-        "madc.hi.u32    %8, %9, %17, %8;"                                                          \
-        : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]),              \
-          "+r"(t[i + 5]), "+r"(t[i + 6]), "+r"(t[i + 7]), "+r"(t[i + 8])                           \
-        : "r"(m_), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5),        \
-          "n"(P::P6), "n"(P::P7));                                                                 \
-  } while (0)
+// Reduction row: t[i+8] holds the product row's top word and accumulates.
+#define ZKG_WIDE_CHAIN_ACC(t, i, d)                                                              \
+  asm("add.cc.u32  %0, %8, %9;\n\t"                                                              \
+      "addc.cc.u32 %1, %10, %11;\n\t"                                                            \
+      "addc.cc.u32 %2, %12, %13;\n\t"                                                            \
+      "addc.cc.u32 %3, %14, %15;\n\t"                                                            \
+      "addc.cc.u32 %4, %16, %17;\n\t"                                                            \
+      "addc.cc.u32 %5, %18, %19;\n\t"                                                            \
+      "addc.cc.u32 %6, %20, %21;\n\t"                                                            \
+      "addc.u32    %7, %7, %22;"                                                                  \
+      : "=&r"(t[i + 1]), "=&r"(t[i + 2]), "=&r"(t[i + 3]), "=&r"(t[i + 4]), "=&r"(t[i + 5]),      \
+        "=&r"(t[i + 6]), "=&r"(t[i + 7]), "+r"(t[i + 8])                                          \
+      : "r"((uint32_t)d[1]), "r"((uint32_t)(d[0] >> 32)), "r"((uint32_t)d[2]),                    \
+        "r"((uint32_t)(d[1] >> 32)), "r"((uint32_t)d[3]), "r"((uint32_t)(d[2] >> 32)),            \
+        "r"((uint32_t)d[4]), "r"((uint32_t)(d[3] >> 32)), "r"((uint32_t)d[5]),                    \
+        "r"((uint32_t)(d[4] >> 32)), "r"((uint32_t)d[6]), "r"((uint32_t)(d[5] >> 32)),            \
+        "r"((uint32_t)d[7]), "r"((uint32_t)(d[6] >> 32)), "r"((uint32_t)(d[7] >> 32)))
 
-// Returns a * b * 2^-256 mod p (coarsely integrated operand scanning: one product row, then
-// one reduction row, per limb of b; 33 multiply-adds per limb).
+// Returns a * b * 2^-256 mod p.
 template <class P>
 __device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
+  constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
   uint32_t t[17];
 #pragma unroll
   for (int i = 0; i < 8; i++) t[i] = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    ZKG_MAD_ROW(t, i, a.w, b.w[i]);
-    ZKG_RED_ROW(P, t, i);
+    uint64_t d[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] = (uint64_t)a.w[j] * b.w[i] + t[i + j];
+    t[i] = (uint32_t)d[0];
+    ZKG_WIDE_CHAIN_FRESH(t, i, d);
+    const uint32_t m = t[i] * P::INV;  // clears word i
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] = (uint64_t)m * q[j] + t[i + j];
+    ZKG_WIDE_CHAIN_ACC(t, i, d);
   }
   // t[8..15] < 2p: one conditional subtraction.
   Fp<P> s, d;

@@ -180,6 +180,20 @@ __global__ void imad_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
       if (V == 0) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(b), "r"(a[(j + 1) & 7]));
       if (V == 1) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(b), "r"(a[(j + 1) & 7]));
     }
+    if (V == 4) {
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        uint64_t p;
+        asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(p) : "r"(a[j]), "r"(b));
+        a[j] = (uint32_t)p ^ a[j + 1];
+        a[j + 1] = (uint32_t)(p >> 32);
+      }
+    }
+    if (V == 5) {
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        asm volatile("add.cc.u32 %0, %0, %1;\n\taddc.u32 %1, %1, %2;" : "+r"(a[j]), "+r"(a[(j + 3) & 7]) : "r"(b));
+    }
     if (V == 2)
       asm volatile(
           "mad.lo.cc.u32  %0, %0, %8, %1;\n\t"
@@ -226,6 +240,8 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
       case 0: imad_kernel<0><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 1: imad_kernel<1><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 2: imad_kernel<2><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 4: imad_kernel<4><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 5: imad_kernel<5><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       default: mulmod_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
     }
     check_launch("integer pipe benchmark");
@@ -244,8 +260,10 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   double threads_total = (double)blocks * threads;
-  // variants 0-2: 8 multiply-adds per step; 3: 2 Fq products per step.
-  double ops = threads_total * iters * (variant == 3 ? 2.0 : 8.0);
+  // variants 0-2: 8 multiply-adds per step; 3: 2 Fq products per step; 4: 4 wide products per
+  // step; 5: 16 carry adds per step.
+  double per = variant == 3 ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
+  double ops = threads_total * iters * per;
   return ops / (best * 1e-3);
 }
 

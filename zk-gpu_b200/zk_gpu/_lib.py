@@ -56,6 +56,7 @@ SIGNATURES = {
     "zkg_msm_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_msm_stage_times": (ctypes.c_int, [vp, ctypes.POINTER(StageTime), ctypes.c_size_t,
                                            ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    "zkg_msm_last_entries": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
     "zkg_ntt_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_ntt_pass_times": (ctypes.c_int, [vp, ctypes.POINTER(StageTime), ctypes.c_size_t,
                                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
