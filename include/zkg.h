@@ -136,6 +136,24 @@ int zkg_ntt_forward(zkg_ntt *ntt, zkg_buf *data);
 /* Ntt::inverse (src/ntt.rs:47-50): in place, includes the 1/n factor. */
 int zkg_ntt_inverse(zkg_ntt *ntt, zkg_buf *data);
 
+/* Largest transform zkg_ntt_noalloc accepts: 2^16 elements. */
+#define ZKG_NTT_NOALLOC_MAX_LOG_N 16
+/* No counterpart in the reference (its Ntt always owns a scratch buffer, src/ntt.rs:31).
+ * In-place Fr NTT of 2^log_n elements (10 <= log_n <= ZKG_NTT_NOALLOC_MAX_LOG_N) in the
+ * caller's device buffer `data` (8 plain words per element, 16-byte aligned), natural order
+ * in and out, the inverse with the 1/n factor; bit-identical to zkg_ntt_forward/inverse.
+ * It allocates no device memory, for callers that cannot call cudaMalloc (a device-memory
+ * budget owned by another allocator, a pipeline where allocation is not allowed): its scratch
+ * is one static device array of 3 MiB that every GPU which loads this library holds until the
+ * process exits. Work is queued on `stream` (a cudaStream_t; NULL = the legacy default stream)
+ * of the calling thread's current device. The first call on a device also resolves the array's
+ * address for that device (cudaGetSymbolAddress) and sets the kernels' shared-memory limit;
+ * make that first call before any stream capture. All calls share the array, which keeps the
+ * last call's contents: calls that overlap on the GPU (different streams, or different host
+ * threads on one device) race and give wrong results; order them on one stream. Larger sizes
+ * are rejected with ZKG_EINVAL ("log_n must be in 10..=16 for zkg_ntt_noalloc, got N"). */
+int zkg_ntt_noalloc(uint32_t log_n, int inverse, uint32_t *data, void *stream);
+
 /* ------------------------------------------------------------------ runtime helpers (no reference counterpart:
  * wgpu hides its queue, launches and staging memory) */
 

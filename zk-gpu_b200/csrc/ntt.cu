@@ -11,7 +11,9 @@
 // The first pass reads the caller's buffer into the plan's scratch, middle passes work in
 // place on the scratch, and the last pass writes back in bit-reversed order (fused with the
 // 1/n scaling for the inverse). Transforms of at most 2^11 elements are one tile in one block.
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -194,3 +196,120 @@ void NttPlan::run(zkg_buf* data, bool inverse) {
 }
 
 }  // namespace zkg
+
+// ------------------------------------------------------------------ allocation-free entry point
+//
+// zkg_ntt_noalloc: the same transform for callers that cannot allocate device memory (code
+// that runs under a memory budget owned by another allocator, inside a stream-ordered
+// pipeline that forbids cudaMalloc, or in a process where only preallocated memory may be
+// touched). Its scratch is a file-scope device array of fixed size instead of plan buffers.
+namespace zkg {
+
+constexpr uint32_t kNoAllocMaxLogN = ZKG_NTT_NOALLOC_MAX_LOG_N;
+constexpr size_t kNoAllocPingPongWords = (size_t)8 << kNoAllocMaxLogN;         // 2 MiB
+constexpr size_t kNoAllocTwiddleWords = (size_t)8 << (kNoAllocMaxLogN - 1);    // 1 MiB
+
+// Every GPU that loads the library holds this array until the process exits. Nothing in it
+// needs clearing: each call writes every word it reads (twiddles first, then pass 0 fills the
+// ping-pong half before later passes read it).
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocPingPongWords + kNoAllocTwiddleWords];
+
+// tw[j] = w^j (Montgomery form) by square-and-multiply over the bits of j.
+__global__ void ntt_twiddles_pow(Fr w, uint32_t count, uint32_t* __restrict__ out) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  Fr acc = Fr::one(), base = w;
+  for (uint32_t e = j; e; e >>= 1) {
+    if (e & 1) acc = acc * base;
+    base = base * base;
+  }
+  store_fe(out + 8 * (size_t)j, acc);
+}
+
+// Device address of g_noalloc_scratch per device, resolved once with that device current (in
+// host code the symbol names a host-side stand-in, not device memory).
+static std::mutex g_noalloc_mutex;
+static uint32_t* g_noalloc_ptr[64];
+
+static uint32_t* noalloc_scratch(int device) {
+  if (device < 0 || device >= 64) fail(ZKG_ENODEV, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
+    const int smem = (int)((size_t)32 << kTileLog);
+    check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+               "ntt smem attribute");
+    check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+               "ntt smem attribute");
+    g_noalloc_ptr[device] = static_cast<uint32_t*>(p);
+  }
+  return g_noalloc_ptr[device];
+}
+
+static void ntt_noalloc(uint32_t log_n, int inverse, uint32_t* data, cudaStream_t s) {
+  if (log_n < 10 || log_n > kNoAllocMaxLogN)
+    fail(ZKG_EINVAL, "log_n must be in 10..=" + std::to_string(kNoAllocMaxLogN) + " for zkg_ntt_noalloc, got " +
+                         std::to_string(log_n));
+  if (!data) fail(ZKG_EINVAL, "data is NULL");
+  if ((reinterpret_cast<uintptr_t>(data) & 15) != 0) fail(ZKG_EINVAL, "data must be 16-byte aligned");
+  int device = 0;
+  check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  uint32_t* scratch = noalloc_scratch(device);
+  uint32_t* pingpong = scratch;
+  uint32_t* tw = scratch + kNoAllocPingPongWords;
+
+  const host::Field& f = host::fr();
+  const size_t n = (size_t)1 << log_n;
+  host::U256 w = host::root_of_unity(log_n);
+  if (inverse) w = host::inverse(w, f);
+  Fr wm, scale;
+  host::words32(w, wm.w);
+  host::words32(host::inverse(host::to_mont(host::U256{{(uint64_t)n, 0, 0, 0}}, f), f), scale.w);
+
+  const uint32_t count = (uint32_t)(n / 2);
+  ntt_twiddles_pow<<<grid_for(count, 256), 256, 0, s>>>(wm, count, tw);
+  check_launch("ntt_twiddles_pow");
+
+  // Same pass split and kernels as NttPlan (fixed arrays, no host allocation either).
+  uint32_t passes[4], np = 0;
+  if (log_n <= kTileLog) {
+    passes[np++] = log_n;
+  } else {
+    uint32_t p = (log_n + kMaxStagesPerPass - 1) / kMaxStagesPerPass;
+    for (uint32_t i = 0; i < p; i++) passes[np++] = log_n / p + (i < log_n % p ? 1u : 0u);
+  }
+  const uint32_t tl = log_n < kTileLog ? log_n : kTileLog;
+  const unsigned tiles = 1u << (log_n - tl);
+  const size_t smem = (size_t)32 << tl;
+  uint32_t done = 0;
+  for (uint32_t i = 0; i < np; i++) {
+    const uint32_t st = passes[i];
+    const uint32_t lm = log_n - done - st;
+    const bool last = i + 1 == np;
+    const uint32_t* src = i == 0 ? data : pingpong;
+    uint32_t* dst = last ? data : pingpong;
+    const int scale_flag = last && inverse;
+    if (last)
+      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+    else
+      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+    check_launch("ntt_pass");
+    done += st;
+  }
+}
+
+}  // namespace zkg
+
+extern "C" int zkg_ntt_noalloc(uint32_t log_n, int inverse, uint32_t* data, void* stream) {
+  try {
+    zkg::ntt_noalloc(log_n, inverse, data, static_cast<cudaStream_t>(stream));
+    return ZKG_OK;
+  } catch (const zkg::Error& e) {
+    zkg::set_error(e.msg);
+    return e.code;
+  } catch (...) {
+    zkg::set_error("unexpected internal error");
+    return ZKG_ECUDA;
+  }
+}

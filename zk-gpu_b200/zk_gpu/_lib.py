@@ -49,6 +49,7 @@ SIGNATURES = {
     "zkg_ntt_log_n": (ctypes.c_uint32, [vp]),
     "zkg_ntt_forward": (ctypes.c_int, [vp, vp]),
     "zkg_ntt_inverse": (ctypes.c_int, [vp, vp]),
+    "zkg_ntt_noalloc": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, vp, vp]),
     "zkg_ctx_stream": (vp, [vp]),
     "zkg_launch_count": (ctypes.c_uint64, []),
     "zkg_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(vp)]),
