@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--log-msm-small", type=int, default=20)
     ap.add_argument("--log-ntt", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the batched-vs-plain request stream")
+    ap.add_argument("--serving-rates", default="2,20,60,200", help="Poisson arrival rates (req/s)")
+    ap.add_argument("--serving-lanes", type=int, default=8)
     return ap.parse_args()
 
 
@@ -357,11 +360,74 @@ def run_ours(a, d: Dist) -> dict | None:
         "clocks": clk,
         "bit_exact": {"ntt_round_trip": round_trip, "e2e_round_trip": e2e_ok},
     }
+    if not a.no_serving:
+        out["serving"] = run_serving(a, gpu)
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"], checks = cpu_baseline(a, gpu, bases, k, s20_host, s24_host, x_host, res20, res24,
                                                    ntt_fwd)
         out["bit_exact"].update(checks)
     del msm24, msm20, ntt
+    return out
+
+
+# ---------------------------------------------------------------- served vs plain request stream
+
+SERVING_KEYS = (18, 20, 21, 22)  # resident proving keys, log2 of their sizes
+SERVING_K = (14, 22)             # circuit size m = 2^k, k uniform over these integers
+
+
+def run_serving(a, gpu) -> dict:
+    """The Groth16-shaped stream through the plain server (one request at a time, operations
+    launched one by one) and the served one (lanes, graphs, continuous batching, HBM-budget
+    admission), same requests, same Poisson arrival times per rate."""
+    from zk_gpu import Group
+    from zk_gpu.serving import ProofInputs, Server, run_stream
+    from zk_gpu.synthetic import generator_multiples, uniform_scalars
+
+    keys = []
+    for lk in SERVING_KEYS:
+        n = 1 << lk
+        g1 = generator_multiples(gpu, Group.G1, uniform_scalars(n, 700 + lk), mont256=True)
+        g2 = generator_multiples(gpu, Group.G2, uniform_scalars(n, 800 + lk), mont256=True)
+        keys.append((n, g1, g2))
+    # one input set per circuit size, reused by every request of that size
+    pool = {}
+    for k in range(SERVING_K[0], SERVING_K[1] + 1):
+        m = 1 << k
+        req = ProofInputs(k)
+        g1 = [uniform_scalars(m, 900 + 3 * k + j) for j in range(3)]
+        g1[2] = g1[2][: 8 * (m - 1024)]
+        polys = [uniform_scalars(2 * m, 950 + 3 * k + j) for j in range(3)]
+        pool[k] = req.fill(g1, uniform_scalars(m, 990 + k), polys)
+    rates = [float(r) for r in a.serving_rates.split(",") if r]
+    out = {"workload": "Groth16-shaped requests: m = 2^k, k uniform in {14..22}; 3 G1 MSMs (m, m, m-1024) + "
+                       "1 G2 MSM (m) on resident keys 2^18/2^20/2^21/2^22 + 7 Fr NTTs of 2m with coset shifts "
+                       "and the quotient; Poisson arrivals",
+           "lanes": a.serving_lanes, "points": []}
+    servers = {}
+    for mode in ("plain", "batched"):
+        sv = Server(gpu, lanes=a.serving_lanes, plain=(mode == "plain"))
+        for n, g1, g2 in keys:
+            sv.add_key(n, g1, g2)
+        # warm every size class once (slot creation, graph capture) outside the timing
+        for k in sorted(pool):
+            sv.wait(sv.submit(pool[k]))
+        servers[mode] = sv
+    for rate in rates:
+        rng = np.random.default_rng(int(rate * 1000) + 17)
+        count = int(max(18, min(72, rate * 3)))
+        ks = rng.integers(SERVING_K[0], SERVING_K[1] + 1, size=count)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
+        point = {"rate_req_per_s": rate, "requests": count}
+        for mode in ("plain", "batched"):
+            r = run_stream(servers[mode], [pool[int(k)] for k in ks], arrivals)
+            point[mode] = {key: round(v, 3) for key, v in r.items() if key != "requests"}
+        point["throughput_ratio"] = round(point["batched"]["req_per_s"] / point["plain"]["req_per_s"], 3)
+        out["points"].append(point)
+    for sv in servers.values():
+        sv.close()
+    top = out["points"][-1]
+    out["max_rate_ratio"] = top["throughput_ratio"]
     return out
 
 

@@ -32,6 +32,9 @@ typedef struct zkg_ctx zkg_ctx; /* gpu::Gpu                           src/gpu.rs
 typedef struct zkg_buf zkg_buf; /* wgpu::Buffer of u32 words          src/gpu.rs:57-69  */
 typedef struct zkg_msm zkg_msm; /* msm::Msm plan                      src/msm.rs:25-37  */
 typedef struct zkg_ntt zkg_ntt; /* ntt::Ntt plan                      src/ntt.rs:14-20  */
+typedef struct zkg_coset zkg_coset;
+typedef struct zkg_batch zkg_batch; /* batched graph launch (no reference type, see below) */
+typedef struct zkg_server zkg_server; /* proving-request server (no reference type, see below) */ /* coset shift by fixed g (no reference type, see below) */
 
 enum zkg_status {
   ZKG_OK = 0,
@@ -100,6 +103,11 @@ int zkg_msm_new(zkg_ctx *ctx, int group, size_t n, uint32_t c, uint32_t item_poi
 void zkg_msm_free(zkg_msm *msm);
 /* Msm::group (src/msm.rs:267-269) */
 int zkg_msm_group(const zkg_msm *msm);
+/* Tuning knobs of a plan (no reference counterpart): the accumulation kernel's form, 0 = field
+ * products inlined, 1 = products through one out-of-line function (smaller code; default).
+ * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
+int zkg_msm_set_variant(zkg_msm *msm, int variant);
+int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,
  * Montgomery form), overwritten by the next run. Checks sizes first ("scalars buffer holds ...",
@@ -135,6 +143,102 @@ uint32_t zkg_ntt_log_n(const zkg_ntt *ntt);
 int zkg_ntt_forward(zkg_ntt *ntt, zkg_buf *data);
 /* Ntt::inverse (src/ntt.rs:47-50): in place, includes the 1/n factor. */
 int zkg_ntt_inverse(zkg_ntt *ntt, zkg_buf *data);
+
+/* Coset shift x_i <- x_i * g^i over the first 2^log_n plain Fr elements of a buffer, for a
+ * fixed g < r given as 8 plain words: the distribute-powers step of a Groth16 witness map
+ * between an inverse and a forward transform. The reference leaves it to callers ("coset
+ * shifts ... are simple kernels on top", README.md:229-230); there is no reference function.
+ * zkg_coset_new precomputes two small power tables (about 2^(log_n/2) elements each). */
+int zkg_coset_new(zkg_ctx *ctx, uint32_t log_n, const uint32_t *g, zkg_coset **out);
+void zkg_coset_free(zkg_coset *coset);
+int zkg_coset_shift(zkg_coset *coset, zkg_buf *data);
+
+/* ------------------------------------------------------------------ autotuning
+ * No reference counterpart (its parameters are fixed: default_window, item size, TILE_LOG).
+ * zkg_tune_msm times, on the given inputs, windows c in [default_window(n) - 2, + 2] within
+ * 9..=20, 16..256 points per accumulation thread and both accumulation kernel forms, and writes
+ * up to cap results fastest first (out[0] is the choice; *count receives how many).
+ * zkg_ntt_set_max_stages picks the pass split of a plan (at most max_stages, 6..11, stages per
+ * shared-memory pass); zkg_tune_ntt times each split on `data` (forward + inverse, which leaves
+ * the data unchanged) and returns the best. */
+typedef struct {
+  uint32_t c, item_points;
+  int variant;
+  double ms;
+} zkg_msm_tuning;
+int zkg_tune_msm(zkg_ctx *ctx, int group, size_t n, const zkg_buf *bases, const zkg_buf *scalars, int reps,
+                 zkg_msm_tuning *out, size_t cap, size_t *count);
+int zkg_ntt_set_max_stages(zkg_ntt *ntt, uint32_t max_stages);
+int zkg_tune_ntt(zkg_ctx *ctx, uint32_t log_n, zkg_buf *data, int reps, uint32_t *best_max_stages, double *best_ms);
+
+/* ------------------------------------------------------------------ batched execution
+ * No reference counterpart: the reference submits one command buffer per stage per call
+ * (src/msm.rs:286-298, src/ntt.rs:52-68). A batch records MSMs, NTTs and coset shifts on
+ * lanes (0 <= lane < 64) and captures them into one CUDA graph: operations in a lane run in
+ * order, lanes are independent branches that the device overlaps. One plan may be used in one
+ * lane only (its scratch is its own). zkg_batch_launch replays the graph on the context stream
+ * with a single launch (capturing first if operations were added since the last capture).
+ * Buffers and plans must stay alive while the batch exists. MSM results are copied into
+ * `result` (>= 32 words G1, 64 words G2), so a plan may run several times in its lane. */
+int zkg_batch_new(zkg_ctx *ctx, zkg_batch **out);
+void zkg_batch_free(zkg_batch *batch);
+int zkg_batch_add_msm(zkg_batch *batch, zkg_msm *msm, const zkg_buf *bases, const zkg_buf *scalars, zkg_buf *result,
+                      int lane);
+int zkg_batch_add_ntt(zkg_batch *batch, zkg_ntt *ntt, zkg_buf *data, int inverse, int lane);
+int zkg_batch_add_coset(zkg_batch *batch, zkg_coset *coset, zkg_buf *data, int lane);
+int zkg_batch_capture(zkg_batch *batch);
+int zkg_batch_launch(zkg_batch *batch);
+/* The same operations without a graph: one stream per lane, joined into the context stream. */
+int zkg_batch_run_streams(zkg_batch *batch);
+/* Kernel nodes in the captured graph (0 before the first capture). */
+size_t zkg_batch_kernels(const zkg_batch *batch);
+
+/* ------------------------------------------------------------------ serving
+ * No reference counterpart (its callers issue one call at a time). A server keeps proving keys
+ * resident and runs Groth16-shaped requests: three G1 MSMs (sizes g1_count[0..2] <= m) and one
+ * G2 MSM (m) over the smallest resident key with at least m = 2^log_m points, and a witness-map
+ * chain of seven Fr NTTs of size N = 2m on the evaluation vectors a, b, c:
+ *   p <- forward(shift_g(inverse(p))) for p in a, b, c;  h <- (a*b - c) / (g^N - 1);
+ *   h <- shift_{1/g}(inverse(h)).
+ * Outputs: out_points = 3 G1 XYZZ (32 words each) then 1 G2 XYZZ (64 words); out_h = N elements.
+ * Requests queue FIFO and are admitted when a free slot (plans and buffers of their size) exists
+ * or a new one fits the HBM budget (idle slots of other sizes are evicted); up to `lanes`
+ * requests run at once on separate streams, each as one captured CUDA graph with three parallel
+ * branches (continuous batching). plain = 1 is the one-call-at-a-time path: one request at a
+ * time, operations launched one by one. Host buffers of a request must stay valid until
+ * zkg_server_wait returns for it, and should be page-locked (zkg_host_alloc) for overlap. */
+typedef struct {
+  int lanes;               /* requests on the device at once, 1..64 (plain forces 1) */
+  int plain;               /* 1 = one request at a time, no graphs, no branches */
+  size_t hbm_budget_bytes; /* device memory for slots; 0 = 80% of the free memory at creation */
+  uint32_t coset_g[8];     /* coset generator g, plain Fr words, 0 < g < r */
+} zkg_server_config;
+typedef struct {
+  uint32_t log_m;                 /* 11..26 */
+  const uint32_t *g1_scalars[3];  /* g1_count[j] scalars each, 8 words per scalar */
+  size_t g1_count[3];
+  const uint32_t *g2_scalars;     /* m scalars */
+  const uint32_t *polys[3];       /* a, b, c: N = 2m plain Fr elements each */
+  uint32_t *out_points;           /* 3*32 + 64 words */
+  uint32_t *out_h;                /* N elements (8*N words) */
+} zkg_proof_request;
+typedef struct {
+  double queued_ms, device_ms, total_ms;  /* submit -> admitted -> done */
+} zkg_request_times;
+typedef struct {
+  uint64_t queued, completed, slots, slots_created, slots_evicted;
+  size_t bytes_used, budget;
+} zkg_server_counters;
+int zkg_server_new(zkg_ctx *ctx, const zkg_server_config *config, zkg_server **out);
+/* Waits for every queued request, then frees the server (keys' buffers stay the caller's). */
+void zkg_server_free(zkg_server *server);
+/* A resident proving key: n affine points in G1 and in G2, Montgomery form (as made by
+ * zkg_msm_upload_bases*). The buffers must outlive the server. */
+int zkg_server_add_key(zkg_server *server, size_t n, const zkg_buf *g1_bases, const zkg_buf *g2_bases);
+int zkg_server_submit(zkg_server *server, const zkg_proof_request *request, uint64_t *id);
+/* Blocks until the request is done (timeout_ms < 0: no limit; ZKG_ETIMEDOUT otherwise). */
+int zkg_server_wait(zkg_server *server, uint64_t id, int timeout_ms, zkg_request_times *times);
+int zkg_server_stats(zkg_server *server, zkg_server_counters *stats);
 
 /* Largest transform zkg_ntt_noalloc accepts: 2^16 elements. */
 #define ZKG_NTT_NOALLOC_MAX_LOG_N 16
@@ -184,7 +288,9 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
 /* Throughput probe of the integer multiply-add pipe (the reference's examples/field_bench.rs
  * measures mulmods per second the same way): variant 0 = mad.lo.u32, 1 = mad.hi.u32,
  * 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq Montgomery
- * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds). *ops_per_second receives multiply-adds (or products) per second on the context's
+ * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds),
+ * 6 = Fq products in an alternative form (plain mul.wide products, two add chains per row; it is
+ * first checked on the device against the production product).  *ops_per_second receives multiply-adds (or products) per second on the context's
  * device; the best of five launches over every SM. */
 int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
 

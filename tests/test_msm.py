@@ -281,3 +281,33 @@ def test_full_size_2_24(gpu, kind):
 def test_full_size_other_window(gpu):
     full_size_case(gpu, 20, "uniform", c=13)
     full_size_case(gpu, 20, "r-1", c=18)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_accumulation_variants_agree(gpu, variant):
+    """Both forms of the accumulation kernel (inlined / out-of-line field products)."""
+    for n, c, items, kind in [(20000, 12, None, "uniform"), (5000, 10, 3, "r-1"), (3000, 9, 1, "sparse")]:
+        bases = random_points("G1", 900 + n, n)
+        s = scalar_distribution(n, kind, 901 + n)
+        msm = Msm.with_item_points(gpu, n, c, items) if items else Msm(gpu, n, c)
+        msm.set_variant(variant)
+        assert msm.params()["variant"] == variant
+        got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, Msm.upload_bases(gpu, bases), gpu.buffer(s)), 32)))
+        assert np.array_equal(got, msm_ref("G1", bases, s)), (n, c, items, kind, variant)
+
+
+def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
+    from zk_gpu.autotune import search_msm, tuned_msm
+    monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
+    n = 1 << 14
+    bases = random_points("G1", 950, n)
+    s = random_fr(951, n)
+    bb, sb = Msm.upload_bases(gpu, bases), gpu.buffer(s)
+    results = search_msm(gpu, Group.G1, n, bb, sb, reps=1)
+    assert results and results == sorted(results, key=lambda r: r["ms"])
+    assert {r["variant"] for r in results} == {0, 1}
+    msm = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)
+    again = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)  # from the cache
+    assert msm.params() == again.params()
+    got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, bb, sb), 32)))
+    assert np.array_equal(got, msm_ref("G1", bases, s))

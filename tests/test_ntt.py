@@ -123,3 +123,60 @@ def test_plan_can_be_reused(gpu):
     for i in reversed(range(4)):
         assert np.array_equal(gpu_ntt(gpu, ntt, inputs[i]), first[i]), f"second run of input {i} differs"
     assert np.array_equal(gpu_ntt(gpu, Ntt(gpu, log_n), inputs[0]), first[0])
+
+
+COSET_G = 7  # Fr's multiplicative generator, the usual coset offset of a Groth16 witness map
+
+
+@pytest.mark.parametrize("log_n", [10, 14, 20])
+def test_coset_shift_matches_oracle(gpu, log_n):
+    from zk_gpu import CosetShift
+    x = random_fr(300 + log_n, 1 << log_n)
+    buf = gpu.buffer(x)
+    CosetShift(gpu, log_n, COSET_G).shift(gpu, buf)
+    g = np.array(bn254.words32(COSET_G), dtype=np.uint32)
+    assert np.array_equal(gpu.read(buf, x.size), cpu.coset_shift(x, g))
+
+
+def test_coset_evaluation_chain(gpu):
+    """inverse -> coset shift -> forward (evaluations on the coset g*H), as the witness map does."""
+    from zk_gpu import CosetShift
+    log_n = 16
+    x = random_fr(400, 1 << log_n)
+    ntt = Ntt(gpu, log_n)
+    buf = gpu.buffer(x)
+    ntt.inverse(gpu, buf)
+    CosetShift(gpu, log_n, COSET_G).shift(gpu, buf)
+    ntt.forward(gpu, buf)
+    g = np.array(bn254.words32(COSET_G), dtype=np.uint32)
+    want = cpu.ntt(cpu.coset_shift(cpu.ntt(x, True), g))
+    assert np.array_equal(gpu.read(buf, x.size), want)
+    # and back: inverse, shift by g^-1, forward returns the input
+    ntt.inverse(gpu, buf)
+    CosetShift(gpu, log_n, pow(COSET_G, R - 2, R)).shift(gpu, buf)
+    ntt.forward(gpu, buf)
+    assert np.array_equal(gpu.read(buf, x.size), x)
+
+
+def test_coset_rejects_bad_generator(gpu):
+    from zk_gpu import CosetShift, ZkGpuError
+    with pytest.raises(ZkGpuError, match="below r"):
+        CosetShift(gpu, 12, R)
+
+
+def test_every_pass_split_is_exact(gpu, tmp_path, monkeypatch):
+    from zk_gpu import lib
+    from zk_gpu._lib import check
+    from zk_gpu.autotune import tuned_ntt
+    log_n = 20
+    x = random_fr(500, 1 << log_n)
+    want = cpu.ntt(x)
+    for s in range(6, 12):
+        ntt = Ntt(gpu, log_n)
+        check(lib().zkg_ntt_set_max_stages(ntt.handle, s))
+        assert np.array_equal(gpu_ntt(gpu, ntt, x), want), f"max_stages = {s}"
+        assert np.array_equal(gpu_ntt(gpu, ntt, want, inverse=True), x), f"max_stages = {s}"
+    monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
+    buf = gpu.buffer(x)
+    ntt = tuned_ntt(gpu, log_n, buf, reps=1)
+    assert np.array_equal(gpu_ntt(gpu, ntt, x), want)

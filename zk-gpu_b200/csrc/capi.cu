@@ -4,11 +4,14 @@
 #include <new>
 #include <string>
 
+#include "batch.hpp"
 #include "host_field.hpp"
 #include "msm.hpp"
 #include "ntt.hpp"
 #include "runtime.hpp"
+#include "server.hpp"
 #include "testing.hpp"
+#include "tuning.hpp"
 
 namespace zkg {
 
@@ -241,6 +244,23 @@ void zkg_msm_free(zkg_msm* msm) {
 
 int zkg_msm_group(const zkg_msm* msm) { return msm ? msm->plan.group : 0; }
 
+int zkg_msm_set_variant(zkg_msm* msm, int variant) {
+  return guard([&] {
+    need(msm, "msm");
+    if (variant < 0 || variant > 1) fail(ZKG_EINVAL, "accumulation variant must be 0 or 1");
+    msm->plan.acc_variant = variant;
+  });
+}
+
+int zkg_msm_params(const zkg_msm* msm, uint32_t* c, uint32_t* item_points, int* variant) {
+  return guard([&] {
+    need(msm, "msm");
+    if (c) *c = msm->plan.c;
+    if (item_points) *item_points = msm->plan.seg_len;
+    if (variant) *variant = msm->plan.acc_variant;
+  });
+}
+
 int zkg_msm_run(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, const zkg_buf** result) {
   return guard([&] {
     need(msm, "msm");
@@ -430,8 +450,184 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 5) fail(ZKG_EINVAL, "variant must be 0..5");
+    if (variant < 0 || variant > 6) fail(ZKG_EINVAL, "variant must be 0..6");
     *ops_per_second = bench_integer_pipe(ctx, variant);
+  });
+}
+
+int zkg_coset_new(zkg_ctx* ctx, uint32_t log_n, const uint32_t* g, zkg_coset** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(g, "g");
+    need(out, "out");
+    *out = nullptr;
+    *out = new zkg_coset(ctx, log_n, g);
+  });
+}
+
+void zkg_coset_free(zkg_coset* c) {
+  if (!c) return;
+  cudaSetDevice(c->shift.ctx->device);
+  cudaStreamSynchronize(c->shift.ctx->stream);
+  delete c;
+}
+
+int zkg_coset_shift(zkg_coset* c, zkg_buf* data) {
+  return guard([&] {
+    need(c, "coset");
+    need(data, "data");
+    c->shift.run(data);
+  });
+}
+
+int zkg_batch_new(zkg_ctx* ctx, zkg_batch** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(out, "out");
+    *out = nullptr;
+    *out = new zkg_batch(ctx);
+  });
+}
+
+void zkg_batch_free(zkg_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->batch.ctx->device);
+  cudaStreamSynchronize(b->batch.ctx->stream);
+  delete b;
+}
+
+int zkg_batch_add_msm(zkg_batch* b, zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, zkg_buf* result,
+                      int lane) {
+  return guard([&] {
+    need(b, "batch");
+    need(msm, "msm");
+    need(bases, "bases");
+    need(scalars, "scalars");
+    b->batch.add_msm(&msm->plan, bases, scalars, result, lane);
+  });
+}
+
+int zkg_batch_add_ntt(zkg_batch* b, zkg_ntt* ntt, zkg_buf* data, int inverse, int lane) {
+  return guard([&] {
+    need(b, "batch");
+    need(ntt, "ntt");
+    need(data, "data");
+    b->batch.add_ntt(&ntt->plan, data, inverse != 0, lane);
+  });
+}
+
+int zkg_batch_add_coset(zkg_batch* b, zkg_coset* c, zkg_buf* data, int lane) {
+  return guard([&] {
+    need(b, "batch");
+    need(c, "coset");
+    need(data, "data");
+    b->batch.add_coset(&c->shift, data, lane);
+  });
+}
+
+int zkg_batch_capture(zkg_batch* b) {
+  return guard([&] {
+    need(b, "batch");
+    b->batch.capture();
+  });
+}
+
+int zkg_batch_launch(zkg_batch* b) {
+  return guard([&] {
+    need(b, "batch");
+    b->batch.launch();
+  });
+}
+
+int zkg_batch_run_streams(zkg_batch* b) {
+  return guard([&] {
+    need(b, "batch");
+    b->batch.run_streams();
+  });
+}
+
+size_t zkg_batch_kernels(const zkg_batch* b) { return b ? b->batch.kernels_per_launch() : 0; }
+
+int zkg_server_new(zkg_ctx* ctx, const zkg_server_config* config, zkg_server** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(config, "config");
+    need(out, "out");
+    *out = nullptr;
+    *out = new zkg_server(ctx, *config);
+  });
+}
+
+void zkg_server_free(zkg_server* s) { delete s; }
+
+int zkg_server_add_key(zkg_server* s, size_t n, const zkg_buf* g1, const zkg_buf* g2) {
+  return guard([&] {
+    need(s, "server");
+    need(g1, "g1_bases");
+    need(g2, "g2_bases");
+    s->server.add_key(n, g1, g2);
+  });
+}
+
+int zkg_server_submit(zkg_server* s, const zkg_proof_request* r, uint64_t* id) {
+  return guard([&] {
+    need(s, "server");
+    need(r, "request");
+    need(id, "id");
+    *id = s->server.submit(*r);
+  });
+}
+
+int zkg_server_wait(zkg_server* s, uint64_t id, int timeout_ms, zkg_request_times* times) {
+  int rc = ZKG_OK;
+  int g = guard([&] {
+    need(s, "server");
+    rc = s->server.wait(id, timeout_ms, times);
+  });
+  if (g != ZKG_OK) return g;
+  if (rc == ZKG_ETIMEDOUT) set_error("request not done within the timeout");
+  return rc;
+}
+
+int zkg_server_stats(zkg_server* s, zkg_server_counters* st) {
+  return guard([&] {
+    need(s, "server");
+    need(st, "stats");
+    s->server.stats(st);
+  });
+}
+
+int zkg_tune_msm(zkg_ctx* ctx, int group, size_t n, const zkg_buf* bases, const zkg_buf* scalars, int reps,
+                 zkg_msm_tuning* out, size_t cap, size_t* count) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(bases, "bases");
+    need(scalars, "scalars");
+    if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+    if (n < 1) fail(ZKG_EINVAL, "an MSM needs at least one point");
+    auto all = tune_msm(ctx, group, n, bases, scalars, reps < 1 ? 1 : reps);
+    size_t k = 0;
+    for (; k < all.size() && k < cap && out; k++) out[k] = all[k];
+    if (count) *count = k;
+  });
+}
+
+int zkg_ntt_set_max_stages(zkg_ntt* ntt, uint32_t max_stages) {
+  return guard([&] {
+    need(ntt, "ntt");
+    if (!ntt->plan.set_max_stages(max_stages) && max_stages != 9)
+      fail(ZKG_EINVAL, "max_stages must be in 6..=11 (one pass below 2^12)");
+  });
+}
+
+int zkg_tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps, uint32_t* best_max_stages, double* best_ms) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(data, "data");
+    auto all = tune_ntt(ctx, log_n, data, reps < 1 ? 1 : reps);
+    if (all.empty()) fail(ZKG_EINVAL, "no pass split applies to this size");
+    if (best_max_stages) *best_max_stages = all[0].first;
+    if (best_ms) *best_ms = all[0].second;
   });
 }
 

@@ -64,6 +64,13 @@ __device__ __forceinline__ Xyzz<F> xyzz_double(const Xyzz<F>& p) {
   return Xyzz<F>{x3, y3, v * p.zz, w * p.zzz};
 }
 
+// The doubling branch of the additions (P = Q) is rare; keeping it out of line keeps the hot
+// addition code small enough for the instruction cache.
+template <class F>
+__device__ __noinline__ Xyzz<F> xyzz_double_call(Xyzz<F> p) {
+  return xyzz_double(p);
+}
+
 // P + Q with Q affine (madd-2008-s).
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const Affine<F>& q) {
@@ -74,7 +81,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const Affin
   F pp = u2 - p.x;
   F r = s2 - p.y;
   if (pp.is_zero()) {
-    if (r.is_zero()) return xyzz_double(p);
+    if (r.is_zero()) return xyzz_double_call(p);
     return xyzz_infinity<F>();
   }
   F ppsq = sqr(pp);
@@ -97,7 +104,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) 
   F pp = u2 - u1;
   F r = s2 - s1;
   if (pp.is_zero()) {
-    if (r.is_zero()) return xyzz_double(p);
+    if (r.is_zero()) return xyzz_double_call(p);
     return xyzz_infinity<F>();
   }
   F ppsq = sqr(pp);

@@ -15,6 +15,7 @@ namespace zkg {
 // Modulus parameters. INV = -p^-1 mod 2^32; ONE = 2^256 mod p (Montgomery one);
 // R2 = 2^512 mod p (to_montgomery multiplier).
 struct FqParams {
+  static constexpr bool kCompact = false;
   static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u;
   static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t INV = 0xe4866389u;
@@ -23,11 +24,20 @@ struct FqParams {
 };
 
 struct FrParams {
+  static constexpr bool kCompact = false;
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u;
   static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t INV = 0xefffffffu;
   static constexpr uint32_t ONE0 = 0x4ffffffbu, ONE1 = 0xac96341cu, ONE2 = 0x9f60cd29u, ONE3 = 0x36fc7695u;
   static constexpr uint32_t ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+};
+
+// Same field, products through one out-of-line function instead of inlined copies. Kernels
+// where few warps run long serial chains (merge, bucket reduction, window combination) use
+// it: a fully inlined point addition is thousands of instructions, and a lone warp walking
+// through straight-line code that size waits on instruction fetch rather than arithmetic.
+struct FqCompactParams : FqParams {
+  static constexpr bool kCompact = true;
 };
 
 template <class P>
@@ -61,6 +71,7 @@ struct Fp {
 
 using Fq = Fp<FqParams>;
 using Fr = Fp<FrParams>;
+using FqC = Fp<FqCompactParams>;
 
 // ------------------------------------------------------------------ add / sub
 
@@ -197,7 +208,7 @@ __device__ __forceinline__ Fp<P> dbl(const Fp<P>& a) {
 
 // Returns a * b * 2^-256 mod p.
 template <class P>
-__device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
+__device__ __forceinline__ Fp<P> mont_mul_inline(const Fp<P>& a, const Fp<P>& b) {
   constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
   uint32_t t[17];
 #pragma unroll
@@ -236,6 +247,106 @@ __device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
 #pragma unroll
   for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
   return r;
+}
+
+// Alternative product for comparison (zkg_bench_integer_pipe variant 6): plain mul.wide products
+// (no 64-bit addend to assemble) and two add chains per row, one for the low halves and one
+// for the high halves one word up; more work on the integer add pipe, less on the multiply
+// pipe. t[i+8] is fresh in a product row and accumulates in a reduction row.
+#define ZKG_ADD_LO_FRESH(t, i, d)                                                                \
+  asm("add.cc.u32  %0, %0, %9;\n\t"                                                              \
+      "addc.cc.u32 %1, %1, %10;\n\t"                                                             \
+      "addc.cc.u32 %2, %2, %11;\n\t"                                                             \
+      "addc.cc.u32 %3, %3, %12;\n\t"                                                             \
+      "addc.cc.u32 %4, %4, %13;\n\t"                                                             \
+      "addc.cc.u32 %5, %5, %14;\n\t"                                                             \
+      "addc.cc.u32 %6, %6, %15;\n\t"                                                             \
+      "addc.cc.u32 %7, %7, %16;\n\t"                                                             \
+      "addc.u32    %8, 0, 0;"                                                                     \
+      : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]), "+r"(t[i + 5]), \
+        "+r"(t[i + 6]), "+r"(t[i + 7]), "=&r"(t[i + 8])                                           \
+      : "r"((uint32_t)d[0]), "r"((uint32_t)d[1]), "r"((uint32_t)d[2]), "r"((uint32_t)d[3]),       \
+        "r"((uint32_t)d[4]), "r"((uint32_t)d[5]), "r"((uint32_t)d[6]), "r"((uint32_t)d[7]))
+#define ZKG_ADD_LO_ACC(t, i, d)                                                                  \
+  asm("add.cc.u32  %0, %0, %9;\n\t"                                                              \
+      "addc.cc.u32 %1, %1, %10;\n\t"                                                             \
+      "addc.cc.u32 %2, %2, %11;\n\t"                                                             \
+      "addc.cc.u32 %3, %3, %12;\n\t"                                                             \
+      "addc.cc.u32 %4, %4, %13;\n\t"                                                             \
+      "addc.cc.u32 %5, %5, %14;\n\t"                                                             \
+      "addc.cc.u32 %6, %6, %15;\n\t"                                                             \
+      "addc.cc.u32 %7, %7, %16;\n\t"                                                             \
+      "addc.u32    %8, %8, 0;"                                                                    \
+      : "+r"(t[i]), "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]), "+r"(t[i + 5]), \
+        "+r"(t[i + 6]), "+r"(t[i + 7]), "+r"(t[i + 8])                                            \
+      : "r"((uint32_t)d[0]), "r"((uint32_t)d[1]), "r"((uint32_t)d[2]), "r"((uint32_t)d[3]),       \
+        "r"((uint32_t)d[4]), "r"((uint32_t)d[5]), "r"((uint32_t)d[6]), "r"((uint32_t)d[7]))
+#define ZKG_ADD_HI(t, i, d)                                                                      \
+  asm("add.cc.u32  %0, %0, %8;\n\t"                                                              \
+      "addc.cc.u32 %1, %1, %9;\n\t"                                                              \
+      "addc.cc.u32 %2, %2, %10;\n\t"                                                             \
+      "addc.cc.u32 %3, %3, %11;\n\t"                                                             \
+      "addc.cc.u32 %4, %4, %12;\n\t"                                                             \
+      "addc.cc.u32 %5, %5, %13;\n\t"                                                             \
+      "addc.cc.u32 %6, %6, %14;\n\t"                                                             \
+      "addc.u32    %7, %7, %15;"                                                                  \
+      : "+r"(t[i + 1]), "+r"(t[i + 2]), "+r"(t[i + 3]), "+r"(t[i + 4]), "+r"(t[i + 5]),           \
+        "+r"(t[i + 6]), "+r"(t[i + 7]), "+r"(t[i + 8])                                            \
+      : "r"((uint32_t)(d[0] >> 32)), "r"((uint32_t)(d[1] >> 32)), "r"((uint32_t)(d[2] >> 32)),    \
+        "r"((uint32_t)(d[3] >> 32)), "r"((uint32_t)(d[4] >> 32)), "r"((uint32_t)(d[5] >> 32)),    \
+        "r"((uint32_t)(d[6] >> 32)), "r"((uint32_t)(d[7] >> 32)))
+
+template <class P>
+__device__ __forceinline__ Fp<P> mont_mul_v2(const Fp<P>& a, const Fp<P>& b) {
+  constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
+  uint32_t t[17];
+#pragma unroll
+  for (int i = 0; i < 8; i++) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint64_t d[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] = (uint64_t)a.w[j] * b.w[i];
+    ZKG_ADD_LO_FRESH(t, i, d);
+    ZKG_ADD_HI(t, i, d);
+    const uint32_t m = t[i] * P::INV;
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] = (uint64_t)m * q[j];
+    ZKG_ADD_LO_ACC(t, i, d);
+    ZKG_ADD_HI(t, i, d);
+  }
+  Fp<P> s, d;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s.w[i] = t[8 + i];
+  uint32_t borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
+        "=&r"(d.w[7]), "=&r"(borrow)
+      : "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7]),
+        "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
+  Fp<P> r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
+  return r;
+}
+
+template <class P>
+__device__ __noinline__ Fp<P> mont_mul_call(Fp<P> a, Fp<P> b) {
+  return mont_mul_inline(a, b);
+}
+
+template <class P>
+__device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
+  if constexpr (P::kCompact) return mont_mul_call<P>(a, b);
+  else return mont_mul_inline(a, b);
 }
 
 template <class P>
@@ -277,29 +388,59 @@ __device__ __forceinline__ void store_fe(void* p, const F& a) {
 // ------------------------------------------------------------------ Fq2 = Fq[u] / (u^2 + 1)
 
 // a + b*u. Karatsuba product in three Fq products, square in two (the reference's G2 prelude,
-// src/group.rs:38-48).
-struct Fq2 {
-  Fq a, b;
-  __device__ __forceinline__ static Fq2 zero() { return Fq2{Fq::zero(), Fq::zero()}; }
-  __device__ __forceinline__ static Fq2 one() { return Fq2{Fq::one(), Fq::zero()}; }
+// src/group.rs:38-48). B is the base field type (Fq, or its compact form FqC).
+template <class B>
+struct Fq2T {
+  B a, b;
+  __device__ __forceinline__ static Fq2T zero() { return Fq2T{B::zero(), B::zero()}; }
+  __device__ __forceinline__ static Fq2T one() { return Fq2T{B::one(), B::zero()}; }
   __device__ __forceinline__ bool is_zero() const { return a.is_zero() && b.is_zero(); }
-  __device__ __forceinline__ bool operator==(const Fq2& o) const { return a == o.a && b == o.b; }
+  __device__ __forceinline__ bool operator==(const Fq2T& o) const { return a == o.a && b == o.b; }
 };
 
-__device__ __forceinline__ Fq2 operator+(const Fq2& x, const Fq2& y) { return Fq2{x.a + y.a, x.b + y.b}; }
-__device__ __forceinline__ Fq2 operator-(const Fq2& x, const Fq2& y) { return Fq2{x.a - y.a, x.b - y.b}; }
-__device__ __forceinline__ Fq2 neg(const Fq2& x) { return Fq2{neg(x.a), neg(x.b)}; }
-__device__ __forceinline__ Fq2 dbl(const Fq2& x) { return Fq2{x.a + x.a, x.b + x.b}; }
-__device__ __forceinline__ Fq2 operator*(const Fq2& x, const Fq2& y) {
-  Fq ac = x.a * y.a;
-  Fq bd = x.b * y.b;
-  Fq cross = (x.a + x.b) * (y.a + y.b);
-  return Fq2{ac - bd, (cross - ac) - bd};
+template <class B>
+__device__ __forceinline__ Fq2T<B> operator+(const Fq2T<B>& x, const Fq2T<B>& y) {
+  return Fq2T<B>{x.a + y.a, x.b + y.b};
 }
-__device__ __forceinline__ Fq2 sqr(const Fq2& x) {
-  Fq ab = x.a * x.b;
-  return Fq2{(x.a + x.b) * (x.a - x.b), ab + ab};
+template <class B>
+__device__ __forceinline__ Fq2T<B> operator-(const Fq2T<B>& x, const Fq2T<B>& y) {
+  return Fq2T<B>{x.a - y.a, x.b - y.b};
 }
+template <class B>
+__device__ __forceinline__ Fq2T<B> neg(const Fq2T<B>& x) {
+  return Fq2T<B>{neg(x.a), neg(x.b)};
+}
+template <class B>
+__device__ __forceinline__ Fq2T<B> dbl(const Fq2T<B>& x) {
+  return Fq2T<B>{x.a + x.a, x.b + x.b};
+}
+template <class B>
+__device__ __forceinline__ Fq2T<B> operator*(const Fq2T<B>& x, const Fq2T<B>& y) {
+  B ac = x.a * y.a;
+  B bd = x.b * y.b;
+  B cross = (x.a + x.b) * (y.a + y.b);
+  return Fq2T<B>{ac - bd, (cross - ac) - bd};
+}
+template <class B>
+__device__ __forceinline__ Fq2T<B> sqr(const Fq2T<B>& x) {
+  B ab = x.a * x.b;
+  return Fq2T<B>{(x.a + x.b) * (x.a - x.b), ab + ab};
+}
+
+using Fq2 = Fq2T<Fq>;
+using Fq2C = Fq2T<FqC>;
+
+// The compact form of a coordinate field (same memory layout).
+template <class F>
+struct CompactOf;
+template <>
+struct CompactOf<Fq> {
+  using type = FqC;
+};
+template <>
+struct CompactOf<Fq2> {
+  using type = Fq2C;
+};
 
 template <class F>
 struct FieldWords;
@@ -312,7 +453,15 @@ struct FieldWords<Fr> {
   static constexpr int value = 8;
 };
 template <>
+struct FieldWords<FqC> {
+  static constexpr int value = 8;
+};
+template <>
 struct FieldWords<Fq2> {
+  static constexpr int value = 16;
+};
+template <>
+struct FieldWords<Fq2C> {
   static constexpr int value = 16;
 };
 
@@ -327,13 +476,23 @@ __device__ __forceinline__ Fr load_elem<Fr>(const uint32_t* p) {
   return load_fe<Fr>(p);
 }
 template <>
+__device__ __forceinline__ FqC load_elem<FqC>(const uint32_t* p) {
+  return load_fe<FqC>(p);
+}
+template <>
 __device__ __forceinline__ Fq2 load_elem<Fq2>(const uint32_t* p) {
   return Fq2{load_fe<Fq>(p), load_fe<Fq>(p + 8)};
+}
+template <>
+__device__ __forceinline__ Fq2C load_elem<Fq2C>(const uint32_t* p) {
+  return Fq2C{load_fe<FqC>(p), load_fe<FqC>(p + 8)};
 }
 
 __device__ __forceinline__ void store_elem(uint32_t* p, const Fq& x) { store_fe(p, x); }
 __device__ __forceinline__ void store_elem(uint32_t* p, const Fr& x) { store_fe(p, x); }
-__device__ __forceinline__ void store_elem(uint32_t* p, const Fq2& x) {
+__device__ __forceinline__ void store_elem(uint32_t* p, const FqC& x) { store_fe(p, x); }
+template <class B>
+__device__ __forceinline__ void store_elem(uint32_t* p, const Fq2T<B>& x) {
   store_fe(p, x.a);
   store_fe(p + 8, x.b);
 }

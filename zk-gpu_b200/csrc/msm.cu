@@ -26,14 +26,14 @@ uint32_t default_window(size_t n) {
   return (uint32_t)c;
 }
 
-// Points accumulated per thread when the caller does not choose: about one wave of 1024
-// threads per SM over the whole sorted array, between 8 and 256 (a power of two).
+// Points accumulated per thread when the caller does not choose, by the number of (point,
+// window) entries; measured on B200 (G1, uniform scalars): 2^16 points best at 16, 2^20 at 64,
+// 2^24 at 128 (fewer, longer segments cost merge work; more, shorter ones cost heads).
 static uint32_t auto_seg_len(size_t n, uint32_t windows) {
-  double entries = (double)n * windows;
-  double target = entries / (148.0 * 1024.0);
-  uint32_t l = 8;
-  while (l < 256 && l < target) l <<= 1;
-  return l;
+  const double entries = (double)n * windows;
+  if (entries < (double)(1u << 22)) return 16;
+  if (entries < (double)(1u << 26)) return 64;
+  return 128;
 }
 
 MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_points)
@@ -139,16 +139,21 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
-      msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr, (uint32_t)slots,
-                                                                 seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      if (acc_variant == 1)
+        msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      else
+        msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr, (uint32_t)slots,
+                                                                   seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
     case kStageMerge: {
+      using FC = typename CompactOf<F>::type;
       size_t len = heads_max;
       for (uint32_t l = 0; l < merge_levels; l++) {
         size_t out_len = (len + kMergeFanIn - 1) / kMergeFanIn;
         int src = l & 1, dst = src ^ 1;
-        msm_merge<F><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)slots, seg_len, l,
+        msm_merge<FC><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)slots, seg_len, l,
                                                             heads[src].ptr, head_keys[src].ptr, heads[dst].ptr,
                                                             head_keys[dst].ptr, buckets.ptr);
         check_launch("msm_merge");
@@ -157,13 +162,14 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       break;
     }
     case kStageReduce: {
+      using FC = typename CompactOf<F>::type;
       const uint32_t* in = buckets.ptr;
       uint32_t in_stride = half;
       for (uint32_t l = 0; l < levels.count; l++) {
         uint32_t m = level_m[l];
         uint32_t chunks = (m + kChunk - 1) / kChunk;
         uint32_t* run_out = runs[l & 1].ptr;
-        msm_reduce_level<F><<<grid_for((size_t)chunks * windows, 128), 128, 0, s>>>(
+        msm_reduce_level<FC><<<grid_for((size_t)chunks * windows, 128), 128, 0, s>>>(
             in, in_stride, m, windows, l == 0 ? slot_start.ptr : nullptr,
             tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(), chunks, run_out, chunks > 1 ? chunks - 1 : 1);
         check_launch("msm_reduce_level");
@@ -172,13 +178,15 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       }
       break;
     }
-    case kStageWindows:
-      msm_window_sums<F><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<F>), s>>>(tots.ptr, levels,
-                                                                                          window_sums.ptr);
+    case kStageWindows: {
+      using FC = typename CompactOf<F>::type;
+      msm_window_sums<FC><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<FC>), s>>>(tots.ptr, levels,
+                                                                                            window_sums.ptr);
       check_launch("msm_window_sums");
       break;
+    }
     case kStageCombine:
-      msm_combine<F><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      msm_combine<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
       check_launch("msm_combine");
       break;
   }

@@ -123,17 +123,25 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   build_twiddles(w_inv, inv_tw);
 
   // Pass split: one tile when it fits, else ceil(log_n / 9) passes of near-equal size.
-  if (log_n <= kTileLog) {
-    passes.push_back(log_n);
-  } else {
-    uint32_t p = (log_n + kMaxStagesPerPass - 1) / kMaxStagesPerPass;
-    for (uint32_t i = 0; i < p; i++) passes.push_back(log_n / p + (i < log_n % p ? 1u : 0u));
-  }
+  set_max_stages(kMaxStagesPerPass);
   const size_t smem = (size_t)32 << (log_n < kTileLog ? log_n : kTileLog);
   check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
   check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
+}
+
+bool NttPlan::set_max_stages(uint32_t ms) {
+  if (ms < 6 || ms > kTileLog) return false;
+  if (log_n <= kTileLog) {
+    passes.assign(1, log_n);
+    return ms == kMaxStagesPerPass;
+  }
+  max_stages = ms;
+  uint32_t p = (log_n + ms - 1) / ms;
+  passes.clear();
+  for (uint32_t i = 0; i < p; i++) passes.push_back(log_n / p + (i < log_n % p ? 1u : 0u));
+  return true;
 }
 
 void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out) {
@@ -193,6 +201,86 @@ void NttPlan::run(zkg_buf* data, bool inverse) {
                         " transform needs " + std::to_string(need));
   use(ctx);
   enqueue(data->ptr, inverse, ctx->stream);
+}
+
+}  // namespace zkg
+
+namespace zkg {
+
+// ------------------------------------------------------------------ coset shift
+//
+// x_i <- x_i * g^i for i < n (the distribute-powers step between the inverse and forward
+// transforms of a Groth16 witness map; SURVEY a'1, README.md:229-230 of the reference names it
+// as a kernel on top). g^i = hi[i >> lo_bits] * lo[i & mask] from two small tables of powers, so
+// each element costs two Fr products and one read and write of 32 bytes.
+__global__ void coset_shift_kernel(uint32_t* __restrict__ data, size_t n, const uint32_t* __restrict__ hi,
+                                   const uint32_t* __restrict__ lo, uint32_t lo_bits) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Fr p = load_fe<Fr>(hi + 8 * (i >> lo_bits)) * load_fe<Fr>(lo + 8 * (i & ((1ull << lo_bits) - 1)));
+  store_fe(data + 8 * i, load_fe<Fr>(data + 8 * i) * p);
+}
+
+CosetShift::CosetShift(zkg_ctx* c, uint32_t log_n_, const uint32_t* g_plain) : ctx(c), log_n(log_n_) {
+  if (log_n < 1 || log_n > 28) fail(ZKG_EINVAL, "log_n must be in 1..=28");
+  use(ctx);
+  const host::Field& f = host::fr();
+  const host::U256 g_raw = host::from_words32(g_plain);
+  if (!(host::geq(f.p, g_raw) && !host::eq(f.p, g_raw))) fail(ZKG_EINVAL, "coset generator must be below r");
+  host::U256 g = host::to_mont(g_raw, f);
+  const size_t n = (size_t)1 << log_n;
+  lo_bits = (log_n + 1) / 2;
+  const size_t lo_len = (size_t)1 << lo_bits;
+  const size_t hi_len = (n + lo_len - 1) / lo_len;
+  std::vector<uint32_t> lo_h = powers_words(g, lo_len);
+  std::vector<uint32_t> hi_h = powers_words(host::pow(g, host::U256{{(uint64_t)lo_len, 0, 0, 0}}, f), hi_len);
+  lo.alloc(lo_h.size(), "coset powers");
+  hi.alloc(hi_h.size(), "coset powers");
+  check_cuda(cudaMemcpyAsync(lo.ptr, lo_h.data(), lo_h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
+  check_cuda(cudaMemcpyAsync(hi.ptr, hi_h.data(), hi_h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
+  check_cuda(cudaStreamSynchronize(ctx->stream), "coset powers");  // host vectors die on return
+}
+
+void CosetShift::enqueue(uint32_t* data, cudaStream_t s) {
+  const size_t n = (size_t)1 << log_n;
+  coset_shift_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, n, hi.ptr, lo.ptr, lo_bits);
+  check_launch("coset_shift_kernel");
+}
+
+void CosetShift::run(zkg_buf* data) {
+  const size_t need = (size_t)8 << log_n;
+  if (data->words < need)
+    fail(ZKG_ESIZE, "data buffer holds " + std::to_string(data->words * 4) + " bytes; a coset shift of 2^" +
+                        std::to_string(log_n) + " elements needs " + std::to_string(need * 4));
+  use(ctx);
+  enqueue(data->ptr, ctx->stream);
+}
+
+// ------------------------------------------------------------------ quotient on the coset
+//
+// a_i <- (a_i * b_i - c_i) * zinv for plain Fr words: the pointwise step of a Groth16 witness
+// map between the forward transforms on the coset g*H and the final inverse (z = g^N - 1 is
+// the vanishing polynomial x^N - 1 evaluated anywhere on that coset). zinv2 holds zinv * R^2
+// (Montgomery form of zinv times R), so three Montgomery products give the plain result:
+//   u = a*b/R, w = c/R, (u - w) * zinv*R^2 / R = (a*b - c) * zinv.
+__global__ void quotient_kernel(uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                const uint32_t* __restrict__ c, size_t n, Fr zinv2) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Fr one = Fr::zero();
+  one.w[0] = 1;
+  Fr u = load_fe<Fr>(a + 8 * i) * load_fe<Fr>(b + 8 * i);
+  Fr w = load_fe<Fr>(c + 8 * i) * one;
+  store_fe(a + 8 * i, (u - w) * zinv2);
+}
+
+void quotient(uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n, const host::U256& zinv, cudaStream_t s) {
+  const host::Field& f = host::fr();
+  Fr z2;
+  host::words32(host::to_mont(host::to_mont(zinv, f), f), z2.w);
+  const size_t n = (size_t)1 << log_n;
+  quotient_kernel<<<grid_for(n, 256), 256, 0, s>>>(a, b, c, n, z2);
+  check_launch("quotient_kernel");
 }
 
 }  // namespace zkg

@@ -16,6 +16,10 @@ struct NttPlan {
   StageTimer timer;  // one stage id per pass
 
   NttPlan(zkg_ctx* ctx, uint32_t log_n);
+  // Splits the stages into passes of at most max_stages (6..11); false if not applicable
+  // (transforms of one tile have a single pass).
+  bool set_max_stages(uint32_t max_stages);
+  uint32_t max_stages = 9;
   // Queues one transform of data (2^log_n elements) on stream s.
   void enqueue(uint32_t* data, bool inverse, cudaStream_t s);
   void run(zkg_buf* data, bool inverse);
@@ -24,7 +28,26 @@ struct NttPlan {
   void build_twiddles(const host::U256& root, DeviceArray& out);
 };
 
+// x_i <- x_i * g^i over the first 2^log_n elements (plain Fr words), g fixed per object.
+struct CosetShift {
+  zkg_ctx* ctx;
+  uint32_t log_n, lo_bits = 0;
+  DeviceArray hi, lo;  // powers g^(k * 2^lo_bits) and g^j, Montgomery form
+  CosetShift(zkg_ctx* ctx, uint32_t log_n, const uint32_t* g_plain);
+  void enqueue(uint32_t* data, cudaStream_t s);
+  void run(zkg_buf* data);
+};
+
+// a_i <- (a_i * b_i - c_i) * zinv over 2^log_n plain Fr elements (zinv a plain value).
+void quotient(uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n, const host::U256& zinv,
+              cudaStream_t s);
+
 }  // namespace zkg
+
+struct zkg_coset {
+  zkg::CosetShift shift;
+  zkg_coset(zkg_ctx* ctx, uint32_t log_n, const uint32_t* g) : shift(ctx, log_n, g) {}
+};
 
 struct zkg_ntt {
   zkg::NttPlan plan;

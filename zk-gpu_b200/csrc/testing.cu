@@ -226,12 +226,49 @@ __global__ void mulmod_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
   if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
 }
 
+// The alternative product (mont_mul_v2), same loop as mulmod_kernel.
+__global__ void mulmod_v2_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
+  Fq x = Fq::one(), y = Fq::one();
+  x.w[0] ^= threadIdx.x + seed;
+  y.w[1] ^= blockIdx.x;
+  Fq z = x;
+  for (uint32_t it = 0; it < iters; it++) {
+    x = mont_mul_v2(x, y);
+    z = mont_mul_v2(z, y);
+  }
+  if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
+}
+
+// Counts threads whose mont_mul_v2 chain differs from the operator* chain (0 expected).
+__global__ void mulmod_compare_kernel(uint32_t* mismatches, uint32_t iters) {
+  Fq x = Fq::one(), y = Fq::one();
+  x.w[0] ^= threadIdx.x * 2654435761u + blockIdx.x;
+  x.w[7] &= 0x0fffffffu;
+  y.w[2] ^= blockIdx.x * 40503u + 7u;
+  y.w[7] &= 0x0fffffffu;
+  Fq u = x, v = x;
+  for (uint32_t it = 0; it < iters; it++) {
+    u = u * y;
+    v = mont_mul_v2(v, y);
+  }
+  if (u != v) atomicAdd(mismatches, 1u);
+}
+
 double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   use(ctx);
   DeviceArray sink;
   sink.alloc(16, "sink");
   const unsigned blocks = (unsigned)ctx->sm_count * 8, threads = 256;
-  const uint32_t iters = variant == 3 ? 256 : 4096;
+  const uint32_t iters = (variant == 3 || variant == 6) ? 256 : 4096;
+  if (variant == 6) {  // the alternative must agree with the production product first
+    check_cuda(cudaMemsetAsync(sink.ptr, 0, 4, ctx->stream), "clear");
+    mulmod_compare_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
+    check_launch("mulmod_compare_kernel");
+    uint32_t bad = 0;
+    check_cuda(cudaMemcpyAsync(&bad, sink.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "compare");
+    if (bad) fail(ZKG_ECUDA, "mont_mul_v2 differs from the production product in " + std::to_string(bad) + " threads");
+  }
   cudaEvent_t a, b;
   check_cuda(cudaEventCreate(&a), "event");
   check_cuda(cudaEventCreate(&b), "event");
@@ -242,6 +279,7 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
       case 2: imad_kernel<2><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 4: imad_kernel<4><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 5: imad_kernel<5><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 6: mulmod_v2_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       default: mulmod_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
     }
     check_launch("integer pipe benchmark");
@@ -262,7 +300,7 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   double threads_total = (double)blocks * threads;
   // variants 0-2: 8 multiply-adds per step; 3: 2 Fq products per step; 4: 4 wide products per
   // step; 5: 16 carry adds per step.
-  double per = variant == 3 ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
+  double per = (variant == 3 || variant == 6) ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
   double ops = threads_total * iters * per;
   return ops / (best * 1e-3);
 }

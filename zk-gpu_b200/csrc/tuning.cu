@@ -1,0 +1,85 @@
+// Autotuner (SURVEY a'3): measures candidate launch parameters on the device and returns the
+// fastest. The reference fixes its parameters (Msm::default_window, src/msm.rs:78-80; item size
+// mean_bucket/4, :99-100; TILE_LOG = 9 for the NTT, src/ntt.rs:9) and sweeps windows by hand
+// (examples/g2_window.rs:50-69); default_window stays the plain form beside the tuned one.
+//
+// MSM candidates: window c in [default - 2, default + 2] within 9..=20, points per accumulation
+// thread in {16, 32, 64, 128, 256}, both accumulation kernel forms. NTT candidates: the most
+// stages per shared-memory pass (passes = ceil(log_n / max_stages)). Each candidate runs once to
+// warm up, then `reps` times between CUDA events; the best mean wins.
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "msm.hpp"
+#include "ntt.hpp"
+#include "tuning.hpp"
+
+namespace zkg {
+
+static double time_ms(cudaStream_t s, int reps, const std::function<void()>& fn) {
+  cudaEvent_t a, b;
+  check_cuda(cudaEventCreate(&a), "event");
+  check_cuda(cudaEventCreate(&b), "event");
+  fn();
+  check_cuda(cudaEventRecord(a, s), "event");
+  for (int i = 0; i < reps; i++) fn();
+  check_cuda(cudaEventRecord(b, s), "event");
+  check_cuda(cudaEventSynchronize(b), "tuning run");
+  float ms = 0;
+  check_cuda(cudaEventElapsedTime(&ms, a, b), "event");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / reps;
+}
+
+std::vector<zkg_msm_tuning> tune_msm(zkg_ctx* ctx, int group, size_t n, const zkg_buf* bases,
+                                     const zkg_buf* scalars, int reps) {
+  use(ctx);
+  const int c0 = (int)default_window(n);
+  std::vector<zkg_msm_tuning> out;
+  for (int c = std::max(9, c0 - 2); c <= std::min(20, c0 + 2); c++) {
+    const uint32_t windows = (255 + c - 1) / c;
+    for (uint32_t L : {16u, 32u, 64u, 128u, 256u}) {
+      // keep at least a few waves of threads on 148 SMs
+      if ((double)n * windows / L < 148.0 * 256 && L > 16) continue;
+      std::unique_ptr<MsmPlan> plan;
+      try {
+        plan.reset(new MsmPlan(ctx, group, n, (uint32_t)c, L));
+      } catch (const Error& e) {
+        if (e.code == ZKG_ENOMEM) {
+          cudaGetLastError();
+          continue;
+        }
+        throw;
+      }
+      plan->check_buffers(bases, scalars);
+      for (int v = 0; v <= 1; v++) {
+        plan->acc_variant = v;
+        double ms = time_ms(ctx->stream, reps, [&] { plan->enqueue(bases->ptr, scalars->ptr, ctx->stream); });
+        out.push_back(zkg_msm_tuning{(uint32_t)c, L, v, ms});
+      }
+    }
+  }
+  std::sort(out.begin(), out.end(), [](const zkg_msm_tuning& a, const zkg_msm_tuning& b) { return a.ms < b.ms; });
+  return out;
+}
+
+std::vector<std::pair<uint32_t, double>> tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps) {
+  use(ctx);
+  std::unique_ptr<NttPlan> plan(new NttPlan(ctx, log_n));
+  if (data->words < ((size_t)8 << log_n)) fail(ZKG_ESIZE, "data buffer too small for the transform");
+  std::vector<std::pair<uint32_t, double>> out;
+  for (uint32_t s = 6; s <= 11; s++) {
+    if (!plan->set_max_stages(s)) continue;
+    double ms = time_ms(ctx->stream, reps, [&] {
+      plan->enqueue(data->ptr, false, ctx->stream);
+      plan->enqueue(data->ptr, true, ctx->stream);
+    });
+    out.push_back({s, ms / 2});
+  }
+  std::sort(out.begin(), out.end(), [](auto& a, auto& b) { return a.second < b.second; });
+  return out;
+}
+
+}  // namespace zkg

@@ -15,11 +15,12 @@ msm, ntt), over the C ABI in include/zkg.h:
 Argument errors raise ZkGpuError with the reference's panic text.
 """
 from ._lib import ZkGpuError, lib
+from .batch import Batch
 from .gpu import Buffer, Gpu
 from .group import Group
 from .msm import Msm, xyzz_to_affine, xyzz_to_affine_g2
-from .ntt import Ntt
+from .ntt import CosetShift, Ntt
 from . import host
 
-__all__ = ["Buffer", "Gpu", "Group", "Msm", "Ntt", "ZkGpuError", "host", "lib", "xyzz_to_affine",
+__all__ = ["Batch", "Buffer", "CosetShift", "Gpu", "Group", "Msm", "Ntt", "ZkGpuError", "host", "lib", "xyzz_to_affine",
            "xyzz_to_affine_g2"]

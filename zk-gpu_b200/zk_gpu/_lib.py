@@ -18,6 +18,32 @@ class StageTime(ctypes.Structure):
     _fields_ = [("stage", ctypes.c_char * 32), ("ms", ctypes.c_double)]
 
 
+class MsmTuning(ctypes.Structure):
+    _fields_ = [("c", ctypes.c_uint32), ("item_points", ctypes.c_uint32), ("variant", ctypes.c_int),
+                ("ms", ctypes.c_double)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_int), ("plain", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("coset_g", ctypes.c_uint32 * 8)]
+
+
+class ProofRequest(ctypes.Structure):
+    _fields_ = [("log_m", ctypes.c_uint32), ("g1_scalars", ctypes.c_void_p * 3), ("g1_count", ctypes.c_size_t * 3),
+                ("g2_scalars", ctypes.c_void_p), ("polys", ctypes.c_void_p * 3), ("out_points", ctypes.c_void_p),
+                ("out_h", ctypes.c_void_p)]
+
+
+class RequestTimes(ctypes.Structure):
+    _fields_ = [("queued_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("slots", ctypes.c_uint64),
+                ("slots_created", ctypes.c_uint64), ("slots_evicted", ctypes.c_uint64),
+                ("bytes_used", ctypes.c_size_t), ("budget", ctypes.c_size_t)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/zkg.h
 SIGNATURES = {
     "zkg_last_error": (ctypes.c_char_p, []),
@@ -39,6 +65,9 @@ SIGNATURES = {
                                    ctypes.POINTER(vp)]),
     "zkg_msm_free": (None, [vp]),
     "zkg_msm_group": (ctypes.c_int, [vp]),
+    "zkg_msm_set_variant": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_params": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_int)]),
     "zkg_msm_run": (ctypes.c_int, [vp, vp, vp, ctypes.POINTER(vp)]),
     "zkg_msm_profile": (ctypes.c_int, [vp, vp, vp, ctypes.POINTER(StageTime), ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_size_t)]),
@@ -49,6 +78,29 @@ SIGNATURES = {
     "zkg_ntt_log_n": (ctypes.c_uint32, [vp]),
     "zkg_ntt_forward": (ctypes.c_int, [vp, vp]),
     "zkg_ntt_inverse": (ctypes.c_int, [vp, vp]),
+    "zkg_coset_new": (ctypes.c_int, [vp, ctypes.c_uint32, u32p, ctypes.POINTER(vp)]),
+    "zkg_coset_free": (None, [vp]),
+    "zkg_coset_shift": (ctypes.c_int, [vp, vp]),
+    "zkg_batch_new": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+    "zkg_batch_free": (None, [vp]),
+    "zkg_batch_add_msm": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int]),
+    "zkg_batch_add_ntt": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_int]),
+    "zkg_batch_add_coset": (ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+    "zkg_batch_capture": (ctypes.c_int, [vp]),
+    "zkg_batch_launch": (ctypes.c_int, [vp]),
+    "zkg_batch_run_streams": (ctypes.c_int, [vp]),
+    "zkg_batch_kernels": (ctypes.c_size_t, [vp]),
+    "zkg_server_new": (ctypes.c_int, [vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+    "zkg_server_free": (None, [vp]),
+    "zkg_server_add_key": (ctypes.c_int, [vp, ctypes.c_size_t, vp, vp]),
+    "zkg_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(ProofRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "zkg_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(RequestTimes)]),
+    "zkg_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+    "zkg_tune_msm": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_size_t, vp, vp, ctypes.c_int,
+                                    ctypes.POINTER(MsmTuning), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "zkg_ntt_set_max_stages": (ctypes.c_int, [vp, ctypes.c_uint32]),
+    "zkg_tune_ntt": (ctypes.c_int, [vp, ctypes.c_uint32, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32),
+                                    ctypes.POINTER(ctypes.c_double)]),
     "zkg_ntt_noalloc": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, vp, vp]),
     "zkg_ctx_stream": (vp, [vp]),
     "zkg_launch_count": (ctypes.c_uint64, []),

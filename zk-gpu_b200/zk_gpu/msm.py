@@ -60,6 +60,15 @@ class Msm:
     def group(self) -> Group:
         return self._group
 
+    def set_variant(self, variant: int) -> None:
+        """Accumulation kernel form: 0 inlined field products, 1 out-of-line (smaller code)."""
+        check(lib().zkg_msm_set_variant(self._h, variant))
+
+    def params(self) -> dict:
+        c, items, var = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
+        check(lib().zkg_msm_params(self._h, ctypes.byref(c), ctypes.byref(items), ctypes.byref(var)))
+        return {"c": c.value, "item_points": items.value, "variant": var.value}
+
     def run(self, gpu: Gpu, bases: Buffer, scalars: Buffer) -> Buffer:
         """Msm::run: queue sum(scalars[i] * bases[i]); returns the plan's XYZZ result buffer
         (borrowed: overwritten by the next run)."""

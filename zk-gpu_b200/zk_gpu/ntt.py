@@ -47,3 +47,34 @@ class Ntt:
             self.close()
         except Exception:
             pass
+
+
+class CosetShift:
+    """x_i <- x_i * g^i over the first 2^log_n elements, g a fixed Fr element (int < r)."""
+
+    def __init__(self, gpu: Gpu, log_n: int, g: int):
+        import numpy as np
+
+        from ._lib import u32p
+        words = np.array([(g >> (32 * i)) & 0xFFFFFFFF for i in range(8)], dtype=np.uint32)
+        h = vp()
+        check(lib().zkg_coset_new(gpu.handle, log_n, words.ctypes.data_as(u32p), ctypes.byref(h)))
+        self._h = h.value
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def shift(self, gpu: Gpu, data: Buffer) -> None:
+        check(lib().zkg_coset_shift(self._h, data.handle))
+
+    def close(self) -> None:
+        if self._h:
+            lib().zkg_coset_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
