@@ -37,11 +37,12 @@ import numpy as np  # noqa: E402
 METRIC = "MSM 2^20/2^24 & NTT 2^24 ms, bit-exact; batched vs plain req/s, p50/p99 ms"
 IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m), field.cuh
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
-# ncu DRAM traffic (read + write bytes) per launch, from profiles/*.md (see the file named
-# in each entry); None until captured.
+# ncu DRAM traffic (read + write bytes) per launch. msm_accumulate: captured at 2^22
+# (profiles/msm_accumulate_g1_2^22.md, 7.07 GB) and scaled by the entry count to 2^24 (x4);
+# ntt_pass: captured at 2^24 (profiles/ntt_pass_2^24.md).
 NCU_TRAFFIC = {
-    "msm_accumulate_2^24": None,
-    "ntt_pass_2^24": None,
+    "msm_accumulate_2^24": 28.3e9,
+    "ntt_pass_2^24": 1.96e9,
 }
 
 
@@ -58,6 +59,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-vs-plain request stream")
     ap.add_argument("--serving-rates", default="2,20,60,200", help="Poisson arrival rates (req/s)")
     ap.add_argument("--serving-lanes", type=int, default=8)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run the small profiling case (Fq product probe, G1 MSM 2^22, Fr NTT 2^24 forward) and exit")
     return ap.parse_args()
 
 
@@ -239,6 +242,31 @@ def run_ours(a, d: Dist) -> dict | None:
         check(L.zkg_msm_set_timing(h, 0))
     check(L.zkg_ntt_set_timing(ntt.handle, 0))
 
+    # ---- the same step as one batched graph launch: the two MSMs and the NTT pair on three lanes
+    from zk_gpu import Batch
+    batch = Batch(gpu)
+    r24, r20 = gpu.empty_buffer(32), gpu.empty_buffer(32)
+    batch.add_msm(msm24, bases, s24, r24, lane=0)
+    batch.add_msm(msm20, bases, s20, r20, lane=1)
+    batch.add_ntt(ntt, data, inverse=False, lane=2)
+    batch.add_ntt(ntt, data, inverse=True, lane=2)
+    batch.capture()
+    for _ in range(a.warmup):
+        batch.launch()
+    torch.cuda.synchronize()
+    d.barrier()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    for _ in range(a.steps):
+        batch.launch()
+    b1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = d.max(b0.elapsed_time(b1) / a.steps)
+    batched_ok = bool(np.array_equal(affine_words(xyzz_to_affine(gpu.read(r24, 32))), res24)
+                      and np.array_equal(affine_words(xyzz_to_affine(gpu.read(r20, 32))), res20)
+                      and np.array_equal(gpu.read(data, x_host.size), x_host))
+    batch.close()
+
     # ---- integer-multiply pipe peak (measured here, the roofline denominator for the MSM)
     peaks = {}
     for v, name in enumerate(["mad_lo", "mad_hi", "madc_chain", "fq_mulmod"]):
@@ -357,6 +385,9 @@ def run_ours(a, d: Dist) -> dict | None:
             "d2h_bytes_per_step": int(4 * (32 + 32 + 2 * x_host.size)),
         },
         "gpu_launches": int(launches),
+        "step_batched": {"ms": round(batched_ms, 4), "lanes": 3, "graph_launches_per_step": 1,
+                         "note": "the same step captured as one CUDA graph: MSM 2^24, MSM 2^20 and the NTT pair on "
+                                 "independent lanes", "same_results": batched_ok},
         "clocks": clk,
         "bit_exact": {"ntt_round_trip": round_trip, "e2e_round_trip": e2e_ok},
     }
@@ -514,8 +545,36 @@ def run_reference(a, d: Dist) -> dict | None:
     }
 
 
+def profile_case():
+    """The small case the ncu captures in profiles/ run: one Fq product probe launch set, one
+    G1 MSM 2^22 (device-built bases, uniform scalars) and one Fr NTT 2^24 forward."""
+    from zk_gpu import Gpu, Group, Msm, Ntt, lib
+    from zk_gpu._lib import check
+    from zk_gpu.synthetic import generator_multiples, uniform_scalars
+
+    gpu = Gpu(0)
+    x = ctypes.c_double()
+    check(lib().zkg_bench_integer_pipe(gpu.handle, 3, ctypes.byref(x)))
+    n = 1 << 22
+    bases = generator_multiples(gpu, Group.G1, uniform_scalars(n, 1), mont256=True)
+    s = gpu.buffer(uniform_scalars(n, 2))
+    msm = Msm(gpu, n, Msm.default_window(n))
+    msm.run(gpu, bases, s)
+    gpu.wait()
+    msm.close()
+    bases.free()
+    s.free()
+    buf = gpu.buffer(uniform_scalars(1 << 24, 3))
+    ntt = Ntt(gpu, 24)
+    ntt.forward(gpu, buf)
+    gpu.wait()
+    print("profile case done", flush=True)
+
+
 def main():
     a = parse()
+    if a.profile_case:
+        return profile_case()
     d = Dist(a.gpus)
     try:
         out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)

@@ -104,7 +104,8 @@ void zkg_msm_free(zkg_msm *msm);
 /* Msm::group (src/msm.rs:267-269) */
 int zkg_msm_group(const zkg_msm *msm);
 /* Tuning knobs of a plan (no reference counterpart): the accumulation kernel's form, 0 = field
- * products inlined, 1 = products through one out-of-line function (smaller code; default).
+ * products inlined, 1 = products through one out-of-line function (smaller code),
+ * 2 = out of line, two independent products per call (default).
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
@@ -156,7 +157,7 @@ int zkg_coset_shift(zkg_coset *coset, zkg_buf *data);
 /* ------------------------------------------------------------------ autotuning
  * No reference counterpart (its parameters are fixed: default_window, item size, TILE_LOG).
  * zkg_tune_msm times, on the given inputs, windows c in [default_window(n) - 2, + 2] within
- * 9..=20, 16..256 points per accumulation thread and both accumulation kernel forms, and writes
+ * 9..=20, 16..256 points per accumulation thread and the three accumulation kernel forms, and writes
  * up to cap results fastest first (out[0] is the choice; *count receives how many).
  * zkg_ntt_set_max_stages picks the pass split of a plan (at most max_stages, 6..11, stages per
  * shared-memory pass); zkg_tune_ntt times each split on `data` (forward + inverse, which leaves
@@ -289,8 +290,9 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
  * measures mulmods per second the same way): variant 0 = mad.lo.u32, 1 = mad.hi.u32,
  * 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq Montgomery
  * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds),
- * 6 = Fq products in an alternative form (plain mul.wide products, two add chains per row; it is
- * first checked on the device against the production product).  *ops_per_second receives multiply-adds (or products) per second on the context's
+ * 6 = Fq products in an alternative form (plain mul.wide products, two add chains per row),
+ * 7 / 8 = products mixing the two forms (product rows / reduction rows in the production form);
+ * alternative forms are first checked on the device against the production product.  *ops_per_second receives multiply-adds (or products) per second on the context's
  * device; the best of five launches over every SM. */
 int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
 

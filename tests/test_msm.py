@@ -283,7 +283,7 @@ def test_full_size_other_window(gpu):
     full_size_case(gpu, 20, "r-1", c=18)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_accumulation_variants_agree(gpu, variant):
     """Both forms of the accumulation kernel (inlined / out-of-line field products)."""
     for n, c, items, kind in [(20000, 12, None, "uniform"), (5000, 10, 3, "r-1"), (3000, 9, 1, "sparse")]:
@@ -305,7 +305,7 @@ def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
     bb, sb = Msm.upload_bases(gpu, bases), gpu.buffer(s)
     results = search_msm(gpu, Group.G1, n, bb, sb, reps=1)
     assert results and results == sorted(results, key=lambda r: r["ms"])
-    assert {r["variant"] for r in results} == {0, 1}
+    assert {r["variant"] for r in results} == {0, 1, 2}
     msm = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)
     again = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)  # from the cache
     assert msm.params() == again.params()

@@ -247,7 +247,7 @@ int zkg_msm_group(const zkg_msm* msm) { return msm ? msm->plan.group : 0; }
 int zkg_msm_set_variant(zkg_msm* msm, int variant) {
   return guard([&] {
     need(msm, "msm");
-    if (variant < 0 || variant > 1) fail(ZKG_EINVAL, "accumulation variant must be 0 or 1");
+    if (variant < 0 || variant > 2) fail(ZKG_EINVAL, "accumulation variant must be 0, 1 or 2");
     msm->plan.acc_variant = variant;
   });
 }
@@ -450,7 +450,7 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 6) fail(ZKG_EINVAL, "variant must be 0..6");
+    if (variant < 0 || variant > 8) fail(ZKG_EINVAL, "variant must be 0..8");
     *ops_per_second = bench_integer_pipe(ctx, variant);
   });
 }

@@ -50,18 +50,20 @@ __device__ __forceinline__ Xyzz<F> negate(const Xyzz<F>& p) {
   return Xyzz<F>{p.x, neg(p.y), p.zz, p.zzz};
 }
 
-// 2P (dbl-2008-s-1, a = 0). Infinity stays infinity (ZZ = 0 gives ZZ3 = 0).
+// 2P (dbl-2008-s-1, a = 0). Infinity stays infinity (ZZ = 0 gives ZZ3 = 0). The nine
+// products go in five steps of independent pairs.
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_double(const Xyzz<F>& p) {
   F u = dbl(p.y);
-  F v = sqr(u);
-  F w = u * v;
-  F s = p.x * v;
-  F x2 = sqr(p.x);
+  F v, x2, w, s, m2, wy, zz3, zzz3;
+  mul2(u, u, p.x, p.x, v, x2);
+  mul2(u, v, p.x, v, w, s);
   F m = dbl(x2) + x2;
-  F x3 = sqr(m) - dbl(s);
-  F y3 = m * (s - x3) - w * p.y;
-  return Xyzz<F>{x3, y3, v * p.zz, w * p.zzz};
+  mul2(m, m, w, p.y, m2, wy);
+  F x3 = m2 - dbl(s);
+  mul2(v, p.zz, w, p.zzz, zz3, zzz3);
+  F y3 = m * (s - x3) - wy;
+  return Xyzz<F>{x3, y3, zz3, zzz3};
 }
 
 // The doubling branch of the additions (P = Q) is rare; keeping it out of line keeps the hot
@@ -71,48 +73,50 @@ __device__ __noinline__ Xyzz<F> xyzz_double_call(Xyzz<F> p) {
   return xyzz_double(p);
 }
 
-// P + Q with Q affine (madd-2008-s).
+// P + Q with Q affine (madd-2008-s): ten products in five pairs.
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const Affine<F>& q) {
   if (is_infinity(q)) return p;
   if (is_infinity(p)) return Xyzz<F>{q.x, q.y, F::one(), F::one()};
-  F u2 = q.x * p.zz;
-  F s2 = q.y * p.zzz;
+  F u2, s2;
+  mul2(q.x, p.zz, q.y, p.zzz, u2, s2);
   F pp = u2 - p.x;
   F r = s2 - p.y;
   if (pp.is_zero()) {
     if (r.is_zero()) return xyzz_double_call(p);
     return xyzz_infinity<F>();
   }
-  F ppsq = sqr(pp);
-  F ppp = pp * ppsq;
-  F q_ = p.x * ppsq;
-  F x3 = (sqr(r) - ppp) - dbl(q_);
-  F y3 = r * (q_ - x3) - p.y * ppp;
-  return Xyzz<F>{x3, y3, p.zz * ppsq, p.zzz * ppp};
+  F ppsq, rr, ppp, q_, zz3, zzz3, t, yppp;
+  mul2(pp, pp, r, r, ppsq, rr);
+  mul2(pp, ppsq, p.x, ppsq, ppp, q_);
+  F x3 = (rr - ppp) - dbl(q_);
+  mul2(r, q_ - x3, p.y, ppp, t, yppp);
+  mul2(p.zz, ppsq, p.zzz, ppp, zz3, zzz3);
+  return Xyzz<F>{x3, t - yppp, zz3, zzz3};
 }
 
-// P + Q, both XYZZ (add-2008-s).
+// P + Q, both XYZZ (add-2008-s): fourteen products in seven pairs.
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) {
   if (is_infinity(q)) return p;
   if (is_infinity(p)) return q;
-  F u1 = p.x * q.zz;
-  F u2 = q.x * p.zz;
-  F s1 = p.y * q.zzz;
-  F s2 = q.y * p.zzz;
+  F u1, u2, s1, s2;
+  mul2(p.x, q.zz, q.x, p.zz, u1, u2);
+  mul2(p.y, q.zzz, q.y, p.zzz, s1, s2);
   F pp = u2 - u1;
   F r = s2 - s1;
   if (pp.is_zero()) {
     if (r.is_zero()) return xyzz_double_call(p);
     return xyzz_infinity<F>();
   }
-  F ppsq = sqr(pp);
-  F ppp = pp * ppsq;
-  F q_ = u1 * ppsq;
-  F x3 = (sqr(r) - ppp) - dbl(q_);
-  F y3 = r * (q_ - x3) - s1 * ppp;
-  return Xyzz<F>{x3, y3, (p.zz * q.zz) * ppsq, (p.zzz * q.zzz) * ppp};
+  F ppsq, rr, ppp, q_, zz12, zzz12, t, sppp, zz3, zzz3;
+  mul2(pp, pp, r, r, ppsq, rr);
+  mul2(pp, ppsq, u1, ppsq, ppp, q_);
+  mul2(p.zz, q.zz, p.zzz, q.zzz, zz12, zzz12);
+  F x3 = (rr - ppp) - dbl(q_);
+  mul2(r, q_ - x3, s1, ppp, t, sppp);
+  mul2(zz12, ppsq, zzz12, ppp, zz3, zzz3);
+  return Xyzz<F>{x3, t - sppp, zz3, zzz3};
 }
 
 // ------------------------------------------------------------------ memory format

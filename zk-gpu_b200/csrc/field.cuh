@@ -16,6 +16,7 @@ namespace zkg {
 // R2 = 2^512 mod p (to_montgomery multiplier).
 struct FqParams {
   static constexpr bool kCompact = false;
+  static constexpr bool kPairs = false;
   static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u;
   static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t INV = 0xe4866389u;
@@ -25,6 +26,7 @@ struct FqParams {
 
 struct FrParams {
   static constexpr bool kCompact = false;
+  static constexpr bool kPairs = false;
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u;
   static constexpr uint32_t P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t INV = 0xefffffffu;
@@ -38,6 +40,13 @@ struct FrParams {
 // through straight-line code that size waits on instruction fetch rather than arithmetic.
 struct FqCompactParams : FqParams {
   static constexpr bool kCompact = true;
+};
+
+// Compact, and independent products go two per call (mul2): shorter dependency waits for a
+// lone thread, more registers per thread.
+struct FqCompactPairParams : FqParams {
+  static constexpr bool kCompact = true;
+  static constexpr bool kPairs = true;
 };
 
 template <class P>
@@ -72,6 +81,7 @@ struct Fp {
 using Fq = Fp<FqParams>;
 using Fr = Fp<FrParams>;
 using FqC = Fp<FqCompactParams>;
+using FqCP = Fp<FqCompactPairParams>;
 
 // ------------------------------------------------------------------ add / sub
 
@@ -338,20 +348,115 @@ __device__ __forceinline__ Fp<P> mont_mul_v2(const Fp<P>& a, const Fp<P>& b) {
   return r;
 }
 
+// Mixed forms for comparison (zkg_bench_integer_pipe variants 7 and 8): one row kind with
+// mad.wide + one chain, the other with mul.wide + two chains. PROD_WIDE selects the product rows'
+// form (true: mad.wide), the reduction rows take the other.
+template <class P, bool PROD_WIDE>
+__device__ __forceinline__ Fp<P> mont_mul_mixed(const Fp<P>& a, const Fp<P>& b) {
+  constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
+  uint32_t t[17];
+#pragma unroll
+  for (int i = 0; i < 8; i++) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint64_t d[8];
+    if constexpr (PROD_WIDE) {
+#pragma unroll
+      for (int j = 0; j < 8; j++) d[j] = (uint64_t)a.w[j] * b.w[i] + t[i + j];
+      t[i] = (uint32_t)d[0];
+      ZKG_WIDE_CHAIN_FRESH(t, i, d);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; j++) d[j] = (uint64_t)a.w[j] * b.w[i];
+      ZKG_ADD_LO_FRESH(t, i, d);
+      ZKG_ADD_HI(t, i, d);
+    }
+    const uint32_t m = t[i] * P::INV;
+    if constexpr (PROD_WIDE) {
+#pragma unroll
+      for (int j = 0; j < 8; j++) d[j] = (uint64_t)m * q[j];
+      ZKG_ADD_LO_ACC(t, i, d);
+      ZKG_ADD_HI(t, i, d);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; j++) d[j] = (uint64_t)m * q[j] + t[i + j];
+      ZKG_WIDE_CHAIN_ACC(t, i, d);
+    }
+  }
+  Fp<P> s, d;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s.w[i] = t[8 + i];
+  uint32_t borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
+        "=&r"(d.w[7]), "=&r"(borrow)
+      : "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7]),
+        "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
+  Fp<P> r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
+  return r;
+}
+
+// The product the library uses: product rows as plain mul.wide with two add chains, reduction
+// rows as mad.wide with one chain (measured 49.6 G products/s against 48.5 for mad.wide in both
+// row kinds and 45.4 for mul.wide in both: the mix balances the multiply and add pipes).
+template <class P>
+__device__ __forceinline__ Fp<P> mont_mul_prod(const Fp<P>& a, const Fp<P>& b) {
+  return mont_mul_mixed<P, false>(a, b);
+}
+
 template <class P>
 __device__ __noinline__ Fp<P> mont_mul_call(Fp<P> a, Fp<P> b) {
-  return mont_mul_inline(a, b);
+  return mont_mul_prod(a, b);
 }
 
 template <class P>
 __device__ __forceinline__ Fp<P> operator*(const Fp<P>& a, const Fp<P>& b) {
   if constexpr (P::kCompact) return mont_mul_call<P>(a, b);
-  else return mont_mul_inline(a, b);
+  else return mont_mul_prod(a, b);
 }
 
 template <class P>
 __device__ __forceinline__ Fp<P> sqr(const Fp<P>& a) {
   return a * a;
+}
+
+// Two independent products. In the compact form they share one out-of-line call, so the two
+// dependency chains interleave (a lone thread, as in the window combination, otherwise waits
+// on one product's chain at a time) and half the calls are made.
+template <class P>
+struct FpPair {
+  Fp<P> x, y;
+};
+
+template <class P>
+__device__ __noinline__ FpPair<P> mont_mul2_call(Fp<P> a, Fp<P> b, Fp<P> c, Fp<P> d) {
+  return FpPair<P>{mont_mul_prod(a, b), mont_mul_prod(c, d)};
+}
+
+template <class P>
+__device__ __forceinline__ void mul2(const Fp<P>& a, const Fp<P>& b, const Fp<P>& c, const Fp<P>& d, Fp<P>& r1,
+                                     Fp<P>& r2) {
+  if constexpr (P::kPairs) {
+    FpPair<P> q = mont_mul2_call<P>(a, b, c, d);
+    r1 = q.x;
+    r2 = q.y;
+  } else if constexpr (P::kCompact) {
+    r1 = mont_mul_call<P>(a, b);
+    r2 = mont_mul_call<P>(c, d);
+  } else {
+    r1 = mont_mul_prod(a, b);
+    r2 = mont_mul_prod(c, d);
+  }
 }
 
 // ------------------------------------------------------------------ memory helpers
@@ -427,10 +532,24 @@ __device__ __forceinline__ Fq2T<B> sqr(const Fq2T<B>& x) {
   return Fq2T<B>{(x.a + x.b) * (x.a - x.b), ab + ab};
 }
 
+// Two independent Fq2 products: the three Karatsuba base products of each, paired.
+template <class B>
+__device__ __forceinline__ void mul2(const Fq2T<B>& x, const Fq2T<B>& y, const Fq2T<B>& z, const Fq2T<B>& w,
+                                     Fq2T<B>& r1, Fq2T<B>& r2) {
+  B ac1, ac2, bd1, bd2, cr1, cr2;
+  mul2(x.a, y.a, z.a, w.a, ac1, ac2);
+  mul2(x.b, y.b, z.b, w.b, bd1, bd2);
+  mul2(x.a + x.b, y.a + y.b, z.a + z.b, w.a + w.b, cr1, cr2);
+  r1 = Fq2T<B>{ac1 - bd1, (cr1 - ac1) - bd1};
+  r2 = Fq2T<B>{ac2 - bd2, (cr2 - ac2) - bd2};
+}
+
 using Fq2 = Fq2T<Fq>;
 using Fq2C = Fq2T<FqC>;
+using Fq2CP = Fq2T<FqCP>;
 
-// The compact form of a coordinate field (same memory layout).
+// The compact forms of a coordinate field (same memory layout): out-of-line products one at a
+// time (CompactOf) or two at a time (PairedOf).
 template <class F>
 struct CompactOf;
 template <>
@@ -440,6 +559,16 @@ struct CompactOf<Fq> {
 template <>
 struct CompactOf<Fq2> {
   using type = Fq2C;
+};
+template <class F>
+struct PairedOf;
+template <>
+struct PairedOf<Fq> {
+  using type = FqCP;
+};
+template <>
+struct PairedOf<Fq2> {
+  using type = Fq2CP;
 };
 
 template <class F>
@@ -457,7 +586,15 @@ struct FieldWords<FqC> {
   static constexpr int value = 8;
 };
 template <>
+struct FieldWords<FqCP> {
+  static constexpr int value = 8;
+};
+template <>
 struct FieldWords<Fq2> {
+  static constexpr int value = 16;
+};
+template <>
+struct FieldWords<Fq2CP> {
   static constexpr int value = 16;
 };
 template <>
@@ -480,6 +617,14 @@ __device__ __forceinline__ FqC load_elem<FqC>(const uint32_t* p) {
   return load_fe<FqC>(p);
 }
 template <>
+__device__ __forceinline__ FqCP load_elem<FqCP>(const uint32_t* p) {
+  return load_fe<FqCP>(p);
+}
+template <>
+__device__ __forceinline__ Fq2CP load_elem<Fq2CP>(const uint32_t* p) {
+  return Fq2CP{load_fe<FqCP>(p), load_fe<FqCP>(p + 8)};
+}
+template <>
 __device__ __forceinline__ Fq2 load_elem<Fq2>(const uint32_t* p) {
   return Fq2{load_fe<Fq>(p), load_fe<Fq>(p + 8)};
 }
@@ -491,6 +636,7 @@ __device__ __forceinline__ Fq2C load_elem<Fq2C>(const uint32_t* p) {
 __device__ __forceinline__ void store_elem(uint32_t* p, const Fq& x) { store_fe(p, x); }
 __device__ __forceinline__ void store_elem(uint32_t* p, const Fr& x) { store_fe(p, x); }
 __device__ __forceinline__ void store_elem(uint32_t* p, const FqC& x) { store_fe(p, x); }
+__device__ __forceinline__ void store_elem(uint32_t* p, const FqCP& x) { store_fe(p, x); }
 template <class B>
 __device__ __forceinline__ void store_elem(uint32_t* p, const Fq2T<B>& x) {
   store_fe(p, x.a);

@@ -142,13 +142,16 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       if (acc_variant == 1)
         msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
             bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      else if (acc_variant == 2)
+        msm_accumulate<typename PairedOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else
         msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr, (uint32_t)slots,
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
     case kStageMerge: {
-      using FC = typename CompactOf<F>::type;
+      using FC = typename PairedOf<F>::type;
       size_t len = heads_max;
       for (uint32_t l = 0; l < merge_levels; l++) {
         size_t out_len = (len + kMergeFanIn - 1) / kMergeFanIn;
@@ -162,7 +165,7 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       break;
     }
     case kStageReduce: {
-      using FC = typename CompactOf<F>::type;
+      using FC = typename PairedOf<F>::type;
       const uint32_t* in = buckets.ptr;
       uint32_t in_stride = half;
       for (uint32_t l = 0; l < levels.count; l++) {
@@ -179,14 +182,14 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       break;
     }
     case kStageWindows: {
-      using FC = typename CompactOf<F>::type;
+      using FC = typename PairedOf<F>::type;
       msm_window_sums<FC><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<FC>), s>>>(tots.ptr, levels,
                                                                                             window_sums.ptr);
       check_launch("msm_window_sums");
       break;
     }
     case kStageCombine:
-      msm_combine<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      msm_combine<typename PairedOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
       check_launch("msm_combine");
       break;
   }

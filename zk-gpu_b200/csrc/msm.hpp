@@ -31,8 +31,9 @@ struct MsmPlan {
   uint32_t c, windows = 0, half = 0, seg_len = 0;
   // Accumulation kernel form: 0 = field products inlined, 1 = through one out-of-line product
   // (smaller code: the inlined mixed addition is thousands of instructions and its warps stall
-  // on instruction fetch; measured 17% faster at 2^24). Tunable.
-  int acc_variant = 1;
+  // on instruction fetch; measured 17% faster at 2^24), 2 = out of line, independent products
+  // two per call (a further 5% at 2^20 and 2^24). Tunable.
+  int acc_variant = 2;
   size_t slots = 0, heads_max = 0;
   uint32_t merge_levels = 0, scan_tiles_n = 0;
   ReduceLevels levels;

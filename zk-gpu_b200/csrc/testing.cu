@@ -239,7 +239,21 @@ __global__ void mulmod_v2_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
   if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
 }
 
-// Counts threads whose mont_mul_v2 chain differs from the operator* chain (0 expected).
+template <bool PROD_WIDE>
+__global__ void mulmod_mixed_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
+  Fq x = Fq::one(), y = Fq::one();
+  x.w[0] ^= threadIdx.x + seed;
+  y.w[1] ^= blockIdx.x;
+  Fq z = x;
+  for (uint32_t it = 0; it < iters; it++) {
+    x = mont_mul_mixed<FqParams, PROD_WIDE>(x, y);
+    z = mont_mul_mixed<FqParams, PROD_WIDE>(z, y);
+  }
+  if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
+}
+
+// Counts threads whose alternative-form chain differs from the operator* chain (0 expected).
+template <int FORM>
 __global__ void mulmod_compare_kernel(uint32_t* mismatches, uint32_t iters) {
   Fq x = Fq::one(), y = Fq::one();
   x.w[0] ^= threadIdx.x * 2654435761u + blockIdx.x;
@@ -249,7 +263,9 @@ __global__ void mulmod_compare_kernel(uint32_t* mismatches, uint32_t iters) {
   Fq u = x, v = x;
   for (uint32_t it = 0; it < iters; it++) {
     u = u * y;
-    v = mont_mul_v2(v, y);
+    if (FORM == 6) v = mont_mul_v2(v, y);
+    if (FORM == 7) v = mont_mul_mixed<FqParams, true>(v, y);
+    if (FORM == 8) v = mont_mul_mixed<FqParams, false>(v, y);
   }
   if (u != v) atomicAdd(mismatches, 1u);
 }
@@ -259,15 +275,18 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   DeviceArray sink;
   sink.alloc(16, "sink");
   const unsigned blocks = (unsigned)ctx->sm_count * 8, threads = 256;
-  const uint32_t iters = (variant == 3 || variant == 6) ? 256 : 4096;
-  if (variant == 6) {  // the alternative must agree with the production product first
+  const bool product = variant == 3 || variant >= 6;
+  const uint32_t iters = product ? 256 : 4096;
+  if (variant >= 6) {  // an alternative form must agree with the production product first
     check_cuda(cudaMemsetAsync(sink.ptr, 0, 4, ctx->stream), "clear");
-    mulmod_compare_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
+    if (variant == 6) mulmod_compare_kernel<6><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
+    if (variant == 7) mulmod_compare_kernel<7><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
+    if (variant == 8) mulmod_compare_kernel<8><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
     check_launch("mulmod_compare_kernel");
     uint32_t bad = 0;
     check_cuda(cudaMemcpyAsync(&bad, sink.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     check_cuda(cudaStreamSynchronize(ctx->stream), "compare");
-    if (bad) fail(ZKG_ECUDA, "mont_mul_v2 differs from the production product in " + std::to_string(bad) + " threads");
+    if (bad) fail(ZKG_ECUDA, "an alternative product form differs from the production one in " + std::to_string(bad) + " threads");
   }
   cudaEvent_t a, b;
   check_cuda(cudaEventCreate(&a), "event");
@@ -280,6 +299,8 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
       case 4: imad_kernel<4><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 5: imad_kernel<5><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 6: mulmod_v2_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 7: mulmod_mixed_kernel<true><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 8: mulmod_mixed_kernel<false><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       default: mulmod_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
     }
     check_launch("integer pipe benchmark");
@@ -300,7 +321,7 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   double threads_total = (double)blocks * threads;
   // variants 0-2: 8 multiply-adds per step; 3: 2 Fq products per step; 4: 4 wide products per
   // step; 5: 16 carry adds per step.
-  double per = (variant == 3 || variant == 6) ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
+  double per = product ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
   double ops = threads_total * iters * per;
   return ops / (best * 1e-3);
 }

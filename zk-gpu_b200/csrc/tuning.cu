@@ -54,7 +54,7 @@ std::vector<zkg_msm_tuning> tune_msm(zkg_ctx* ctx, int group, size_t n, const zk
         throw;
       }
       plan->check_buffers(bases, scalars);
-      for (int v = 0; v <= 1; v++) {
+      for (int v = 0; v <= 2; v++) {
         plan->acc_variant = v;
         double ms = time_ms(ctx->stream, reps, [&] { plan->enqueue(bases->ptr, scalars->ptr, ctx->stream); });
         out.push_back(zkg_msm_tuning{(uint32_t)c, L, v, ms});

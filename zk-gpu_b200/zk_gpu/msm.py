@@ -61,7 +61,8 @@ class Msm:
         return self._group
 
     def set_variant(self, variant: int) -> None:
-        """Accumulation kernel form: 0 inlined field products, 1 out-of-line (smaller code)."""
+        """Accumulation kernel form: 0 inlined field products, 1 out-of-line (smaller code),
+        2 out-of-line two at a time."""
         check(lib().zkg_msm_set_variant(self._h, variant))
 
     def params(self) -> dict:
