@@ -36,12 +36,13 @@ import numpy as np  # noqa: E402
 
 METRIC = "MSM 2^20/2^24 & NTT 2^24 ms, bit-exact; batched vs plain req/s, p50/p99 ms"
 IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m), field.cuh
+FP64_PER_MULMOD = 170  # double-precision instructions per Fq product in limb form, field_f64.cuh
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
-# ncu DRAM traffic (read + write bytes) per launch. msm_accumulate: captured at 2^22
-# (profiles/msm_accumulate_g1_2^22.md, 7.07 GB) and scaled by the entry count to 2^24 (x4);
+# ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured at 2^22
+# (profiles/msm_accumulate_f64_g1_2^22.md, 7.05 GB) and scaled by the entry count to 2^24 (x4);
 # ntt_pass: captured at 2^24 (profiles/ntt_pass_2^24.md).
 NCU_TRAFFIC = {
-    "msm_accumulate_2^24": 28.3e9,
+    "msm_accumulate_2^24": 28.2e9,
     "ntt_pass_2^24": 1.96e9,
 }
 
@@ -269,7 +270,8 @@ def run_ours(a, d: Dist) -> dict | None:
 
     # ---- integer-multiply pipe peak (measured here, the roofline denominator for the MSM)
     peaks = {}
-    for v, name in enumerate(["mad_lo", "mad_hi", "madc_chain", "fq_mulmod"]):
+    for v, name in [(0, "mad_lo"), (1, "mad_hi"), (2, "madc_chain"), (3, "fq_mulmod"), (9, "dfma"),
+                    (11, "fq_mulmod_fp64")]:
         x = ctypes.c_double()
         check(L.zkg_bench_integer_pipe(gpu.handle, v, ctypes.byref(x)))
         peaks[name] = x.value
@@ -314,6 +316,8 @@ def run_ours(a, d: Dist) -> dict | None:
     acc_ms = st24.get("accumulate", float("nan"))
     acc_ops = entries.value * MULMODS_PER_MADD * IMAD_PER_MULMOD
     acc_achieved = acc_ops / (acc_ms * 1e-3)
+    acc_fp64 = entries.value * MULMODS_PER_MADD * FP64_PER_MULMOD / (acc_ms * 1e-3)
+    acc_variant = msm24.params()["variant"]
     n_pass = len(stn)
     ntt_pass_ms = sum(stn.values()) / max(n_pass, 1)  # mean pass duration (forward and inverse)
     ntt_bytes = 64 * nn  # each pass reads and writes 32 B per element
@@ -353,7 +357,8 @@ def run_ours(a, d: Dist) -> dict | None:
                       f"msm_2^{a.log_msm_small}": {k: round(v, 4) for k, v in st20.items()},
                       f"ntt_2^{a.log_ntt}": {k: round(v, 4) for k, v in stn.items()}},
         "roofline": {
-            "kernel": f"msm_accumulate<Fq> (G1 MSM 2^{a.log_msm})",
+            "kernel": (f"msm_accumulate_f64 (G1 MSM 2^{a.log_msm}; Fq products on the FP64 pipe)" if acc_variant >= 3
+                       else f"msm_accumulate<Fq> (G1 MSM 2^{a.log_msm})"),
             "bound": "imad",
             "achieved": round(acc_achieved / 1e12, 3),
             "peak": round(imad_peak / 1e12, 3),
@@ -361,9 +366,12 @@ def run_ours(a, d: Dist) -> dict | None:
             "frac": round(acc_achieved / imad_peak, 4),
             "traffic": NCU_TRAFFIC["msm_accumulate_2^24"],
             "algorithmic": f"{entries.value} nonzero digits x {MULMODS_PER_MADD} Fq products x "
-                           f"{IMAD_PER_MULMOD} multiply-adds",
+                           f"{IMAD_PER_MULMOD} 32-bit multiply-adds (the integer-product equivalent of the work)",
             "peak_source": "measured in this run: best of mad.lo / mad.hi / carry-chain probes "
                            "(zkg_bench_integer_pipe)",
+            "fp64_pipe": {"achieved": round(acc_fp64 / 1e12, 3), "peak": round(peaks["dfma"] / 1e12, 3),
+                          "unit": "T FP64 instr/s", "frac": round(acc_fp64 / peaks["dfma"], 4),
+                          "algorithmic": f"{FP64_PER_MULMOD} FP64 instructions per Fq product"},
         },
         "roofline_ntt": {
             "kernel": f"ntt_pass (Fr NTT 2^{a.log_ntt}, {n_pass} passes)",

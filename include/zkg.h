@@ -105,7 +105,9 @@ void zkg_msm_free(zkg_msm *msm);
 int zkg_msm_group(const zkg_msm *msm);
 /* Tuning knobs of a plan (no reference counterpart): the accumulation kernel's form, 0 = field
  * products inlined, 1 = products through one out-of-line function (smaller code),
- * 2 = out of line, two independent products per call (default).
+ * 2 = out of line, two independent products per call, 3 / 4 = G1 only: bucket sums in
+ * double-precision limbs, products on the FP64 pipe, two per call / one per call (ZKG_EINVAL
+ * for G2). Defaults: 4 for G1, 1 for G2.
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
@@ -159,9 +161,13 @@ int zkg_coset_shift(zkg_coset *coset, zkg_buf *data);
  * zkg_tune_msm times, on the given inputs, windows c in [default_window(n) - 2, + 2] within
  * 9..=20, 16..256 points per accumulation thread and the three accumulation kernel forms, and writes
  * up to cap results fastest first (out[0] is the choice; *count receives how many).
- * zkg_ntt_set_max_stages picks the pass split of a plan (at most max_stages, 6..11, stages per
- * shared-memory pass); zkg_tune_ntt times each split on `data` (forward + inverse, which leaves
- * the data unchanged) and returns the best. */
+ * zkg_ntt_set_variant picks a plan's butterfly form: 0 = 32-bit integer products (tiles of 2^11
+ * elements; default), 1 = double-precision limbs, products on the FP64 pipe (tiles of 2^10);
+ * it resets the pass split to the form's default (at most 9 / 8 stages per pass).
+ * zkg_ntt_set_max_stages picks the pass split (at most max_stages, 6..=11 for form 0, 6..=10
+ * for form 1, stages per shared-memory pass); zkg_ntt_params reports form, split and passes.
+ * zkg_tune_ntt times both forms and each split on `data` (forward + inverse, which leaves the
+ * data unchanged) and returns the best. */
 typedef struct {
   uint32_t c, item_points;
   int variant;
@@ -169,8 +175,11 @@ typedef struct {
 } zkg_msm_tuning;
 int zkg_tune_msm(zkg_ctx *ctx, int group, size_t n, const zkg_buf *bases, const zkg_buf *scalars, int reps,
                  zkg_msm_tuning *out, size_t cap, size_t *count);
+int zkg_ntt_set_variant(zkg_ntt *ntt, int variant);
 int zkg_ntt_set_max_stages(zkg_ntt *ntt, uint32_t max_stages);
-int zkg_tune_ntt(zkg_ctx *ctx, uint32_t log_n, zkg_buf *data, int reps, uint32_t *best_max_stages, double *best_ms);
+int zkg_ntt_params(const zkg_ntt *ntt, int *variant, uint32_t *max_stages, uint32_t *passes);
+int zkg_tune_ntt(zkg_ctx *ctx, uint32_t log_n, zkg_buf *data, int reps, int *best_variant, uint32_t *best_max_stages,
+                 double *best_ms);
 
 /* ------------------------------------------------------------------ batched execution
  * No reference counterpart: the reference submits one command buffer per stage per call
@@ -292,7 +301,16 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
  * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds),
  * 6 = Fq products in an alternative form (plain mul.wide products, two add chains per row),
  * 7 / 8 = products mixing the two forms (product rows / reduction rows in the production form);
- * alternative forms are first checked on the device against the production product.  *ops_per_second receives multiply-adds (or products) per second on the context's
+ * 9 = fma.rn.f64 (the double-precision pipe), 10 = the same FMAs interleaved with mul.wide.u32
+ * (counts the FMAs only: equal to 9 when the two pipes issue concurrently), 11 = Fq Montgomery
+ * products on the double-precision pipe (five 52-bit limbs, R = 2^260), 12 = the same with each
+ * column summed as one expression; 13 / 14 = the FMAs of 9 interleaved with mad.lo.u32 / 64-bit adds
+ * (FMAs counted); 15 / 16 / 17 = the double-precision product with the product-phase column adds,
+ * every column add, or the low halves' adds issued as integer multiply-adds by 1; 18 / 19 = one
+ * dependent chain of Fq products on a single thread (integer / double-precision form; products
+ * per second = 1 / latency);
+ * alternative forms are first checked on the device against the production product.
+ * *ops_per_second receives multiply-adds (or products, or FMAs) per second on the context's
  * device; the best of five launches over every SM. */
 int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
 

@@ -16,40 +16,48 @@ pytestmark = pytest.mark.gpu
 R = bn254.R
 
 
-def check(gpu, bases, scalars, c, what):
+def check(gpu, bases, scalars, c, what, variant=None):
     expected = msm_ref("G1", bases, scalars)
     for item_points in (1024, 7):
-        got = gpu_msm(gpu, bases, scalars, (c, item_points))
-        assert np.array_equal(got, expected), f"{what} (n = {scalars.size // 8}, c = {c}, item_points = {item_points})"
+        got = gpu_msm(gpu, bases, scalars, (c, item_points), variant=variant)
+        assert np.array_equal(got, expected), \
+            f"{what} (n = {scalars.size // 8}, c = {c}, item_points = {item_points}, variant = {variant})"
 
 
-def test_random_inputs(gpu):
+# Accumulation kernel forms checked by the edge-case suites: the default, and the G1 forms
+# whose bucket arithmetic runs in double-precision limbs (their own special-case paths).
+EDGE_VARIANTS = [None, 3, 4]
+
+
+@pytest.mark.parametrize("variant", EDGE_VARIANTS)
+def test_random_inputs(gpu, variant):
     for n, c in [(1000, 9), (4096, 10), (20000, 12), (100000, 14)]:
-        check(gpu, random_points("G1", n, n), random_fr(n + 1, n), c, "random")
+        check(gpu, random_points("G1", n, n), random_fr(n + 1, n), c, "random", variant)
 
 
-def test_edge_cases(gpu):
+@pytest.mark.parametrize("variant", EDGE_VARIANTS)
+def test_edge_cases(gpu, variant):
     n, c = 3000, 10
     p = random_points("G1", 1, 1)
     rand = random_points("G1", 2, n)
     rand_s = random_fr(3, n)
-    check(gpu, rand, fr_words([0] * n), c, "all-zero scalars")
-    check(gpu, rand, fr_words([1] * n), c, "all-one scalars (one huge bucket)")
-    check(gpu, rand, fr_words([R - 1] * n), c, "scalars = r - 1")
+    check(gpu, rand, fr_words([0] * n), c, "all-zero scalars", variant)
+    check(gpu, rand, fr_words([1] * n), c, "all-one scalars (one huge bucket)", variant)
+    check(gpu, rand, fr_words([R - 1] * n), c, "scalars = r - 1", variant)
     same = np.tile(p, n)
-    check(gpu, same, rand_s, c, "same base everywhere (forces doublings)")
-    check(gpu, same, fr_words([5] * n), c, "same base, same scalar")
-    check(gpu, rand, fr_words(i % 7 for i in range(n)), c, "tiny scalars")
+    check(gpu, same, rand_s, c, "same base everywhere (forces doublings)", variant)
+    check(gpu, same, fr_words([5] * n), c, "same base, same scalar", variant)
+    check(gpu, rand, fr_words(i % 7 for i in range(n)), c, "tiny scalars", variant)
     with_inf = rand.copy()
     with_inf[16 * 3: 16 * 4] = 0
     with_inf[16 * 100: 16 * 101] = 0
-    check(gpu, with_inf, rand_s, c, "bases containing infinity")
+    check(gpu, with_inf, rand_s, c, "bases containing infinity", variant)
     negp = np.array(bn254.affine_words("G1", bn254.affine_neg(bn254._FqOps, (bn254.from_words32(p[:8]),
                                                                             bn254.from_words32(p[8:])))),
                     dtype=np.uint32)
     cancel = np.concatenate([p, negp, rand[:16 * 8]])
     cs = np.concatenate([rand_s[:8], rand_s[:8], np.zeros(64, dtype=np.uint32)])
-    check(gpu, cancel, cs, c, "cancels to the point at infinity")
+    check(gpu, cancel, cs, c, "cancels to the point at infinity", variant)
 
 
 def test_default_parameters(gpu):
@@ -244,7 +252,7 @@ def test_fuzz(gpu):
 
 # ---------------------------------------------------------------- full sizes
 
-def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0):
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None):
     """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
     uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G."""
     n = 1 << log_n
@@ -258,10 +266,12 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0):
     c = c or Msm.default_window(n)
     base_buf = Msm.upload_bases(gpu, plain)
     msm = Msm(gpu, n, c)
+    if variant is not None:
+        msm.set_variant(variant)
     got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, gpu.buffer(s)), 32)))
     gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
     want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
-    assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}) wrong"
+    assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}, variant = {variant}) wrong"
     # spot check the device-built bases against the CPU
     for i in (0, 1, n - 1):
         assert np.array_equal(plain[16 * i: 16 * i + 16], cpu.generator_multiples("G1", k[8 * i: 8 * i + 8]))
@@ -283,9 +293,17 @@ def test_full_size_other_window(gpu):
     full_size_case(gpu, 20, "r-1", c=18)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"])
+@pytest.mark.parametrize("variant", [3, 4])
+def test_full_size_double_precision_forms(gpu, variant, kind):
+    full_size_case(gpu, 22, kind, variant=variant)
+    full_size_case(gpu, 18, kind, c=16, variant=variant)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_accumulation_variants_agree(gpu, variant):
-    """Both forms of the accumulation kernel (inlined / out-of-line field products)."""
+    """Every form of the accumulation kernel (inlined / out-of-line integer field products,
+    double-precision limbs)."""
     for n, c, items, kind in [(20000, 12, None, "uniform"), (5000, 10, 3, "r-1"), (3000, 9, 1, "sparse")]:
         bases = random_points("G1", 900 + n, n)
         s = scalar_distribution(n, kind, 901 + n)
@@ -305,7 +323,7 @@ def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
     bb, sb = Msm.upload_bases(gpu, bases), gpu.buffer(s)
     results = search_msm(gpu, Group.G1, n, bb, sb, reps=1)
     assert results and results == sorted(results, key=lambda r: r["ms"])
-    assert {r["variant"] for r in results} == {0, 1, 2}
+    assert {r["variant"] for r in results} == {1, 2, 3, 4}
     msm = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)
     again = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)  # from the cache
     assert msm.params() == again.params()

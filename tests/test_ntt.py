@@ -5,7 +5,7 @@ import pytest
 
 from common import fr_words, gpu_ntt, quick, random_fr
 from oracle import bn254, cpu
-from zk_gpu import Ntt
+from zk_gpu import Ntt, ZkGpuError
 
 pytestmark = pytest.mark.gpu
 R = bn254.R
@@ -21,6 +21,18 @@ def test_matches_oracle(gpu, log_n):
     assert np.array_equal(got, cpu.ntt(x)), f"forward NTT mismatch at log_n={log_n}"
     ntt.inverse(gpu, buf)
     assert np.array_equal(gpu.read(buf, x.size), x), f"inverse NTT did not restore the input at log_n={log_n}"
+
+
+@pytest.mark.parametrize("log_n", [10, 11, 13, 16, 20])
+def test_double_precision_form_matches_oracle(gpu, log_n):
+    """The double-precision butterfly form (variant 1) beside the default integer one."""
+    x = random_fr(300 + log_n, 1 << log_n)
+    ntt = Ntt(gpu, log_n)
+    assert ntt.params()["variant"] == 0
+    ntt.set_variant(1)
+    assert ntt.params()["variant"] == 1
+    assert np.array_equal(gpu_ntt(gpu, ntt, x), cpu.ntt(x)), f"log_n={log_n}"
+    assert np.array_equal(gpu_ntt(gpu, ntt, cpu.ntt(x), inverse=True), x), f"log_n={log_n}"
 
 
 @pytest.mark.parametrize("log_n", [24, 26] if not quick() else [24])
@@ -165,17 +177,21 @@ def test_coset_rejects_bad_generator(gpu):
 
 
 def test_every_pass_split_is_exact(gpu, tmp_path, monkeypatch):
-    from zk_gpu import lib
-    from zk_gpu._lib import check
     from zk_gpu.autotune import tuned_ntt
     log_n = 20
     x = random_fr(500, 1 << log_n)
     want = cpu.ntt(x)
-    for s in range(6, 12):
-        ntt = Ntt(gpu, log_n)
-        check(lib().zkg_ntt_set_max_stages(ntt.handle, s))
-        assert np.array_equal(gpu_ntt(gpu, ntt, x), want), f"max_stages = {s}"
-        assert np.array_equal(gpu_ntt(gpu, ntt, want, inverse=True), x), f"max_stages = {s}"
+    for variant, top in ((0, 11), (1, 10)):
+        for s in range(6, top + 1):
+            ntt = Ntt(gpu, log_n)
+            ntt.set_variant(variant)
+            ntt.set_max_stages(s)
+            p = ntt.params()
+            assert (p["variant"], p["max_stages"]) == (variant, s)
+            assert np.array_equal(gpu_ntt(gpu, ntt, x), want), f"variant {variant}, max_stages = {s}"
+            assert np.array_equal(gpu_ntt(gpu, ntt, want, inverse=True), x), f"variant {variant}, max_stages = {s}"
+        with pytest.raises(ZkGpuError):
+            ntt.set_max_stages(top + 1)
     monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
     buf = gpu.buffer(x)
     ntt = tuned_ntt(gpu, log_n, buf, reps=1)

@@ -247,7 +247,8 @@ int zkg_msm_group(const zkg_msm* msm) { return msm ? msm->plan.group : 0; }
 int zkg_msm_set_variant(zkg_msm* msm, int variant) {
   return guard([&] {
     need(msm, "msm");
-    if (variant < 0 || variant > 2) fail(ZKG_EINVAL, "accumulation variant must be 0, 1 or 2");
+    if (variant < 0 || variant > 4) fail(ZKG_EINVAL, "accumulation variant must be 0..4");
+    if (variant >= 3 && msm->plan.group != ZKG_G1) fail(ZKG_EINVAL, "accumulation variants 3 and 4 are for G1 only");
     msm->plan.acc_variant = variant;
   });
 }
@@ -450,7 +451,7 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 8) fail(ZKG_EINVAL, "variant must be 0..8");
+    if (variant < 0 || variant > 19) fail(ZKG_EINVAL, "variant must be 0..19");
     *ops_per_second = bench_integer_pipe(ctx, variant);
   });
 }
@@ -612,22 +613,40 @@ int zkg_tune_msm(zkg_ctx* ctx, int group, size_t n, const zkg_buf* bases, const 
   });
 }
 
-int zkg_ntt_set_max_stages(zkg_ntt* ntt, uint32_t max_stages) {
+int zkg_ntt_set_variant(zkg_ntt* ntt, int variant) {
   return guard([&] {
     need(ntt, "ntt");
-    if (!ntt->plan.set_max_stages(max_stages) && max_stages != 9)
-      fail(ZKG_EINVAL, "max_stages must be in 6..=11 (one pass below 2^12)");
+    if (!ntt->plan.set_variant(variant)) fail(ZKG_EINVAL, "NTT variant must be 0 or 1");
   });
 }
 
-int zkg_tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps, uint32_t* best_max_stages, double* best_ms) {
+int zkg_ntt_set_max_stages(zkg_ntt* ntt, uint32_t max_stages) {
+  return guard([&] {
+    need(ntt, "ntt");
+    if (!ntt->plan.set_max_stages(max_stages))
+      fail(ZKG_EINVAL, "max_stages must be in 6..=" + std::to_string(ntt->plan.tile_log()) + " for this NTT variant");
+  });
+}
+
+int zkg_ntt_params(const zkg_ntt* ntt, int* variant, uint32_t* max_stages, uint32_t* passes) {
+  return guard([&] {
+    need(ntt, "ntt");
+    if (variant) *variant = ntt->plan.variant;
+    if (max_stages) *max_stages = ntt->plan.max_stages;
+    if (passes) *passes = (uint32_t)ntt->plan.passes.size();
+  });
+}
+
+int zkg_tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps, int* best_variant, uint32_t* best_max_stages,
+                 double* best_ms) {
   return guard([&] {
     need(ctx, "ctx");
     need(data, "data");
     auto all = tune_ntt(ctx, log_n, data, reps < 1 ? 1 : reps);
     if (all.empty()) fail(ZKG_EINVAL, "no pass split applies to this size");
-    if (best_max_stages) *best_max_stages = all[0].first;
-    if (best_ms) *best_ms = all[0].second;
+    if (best_variant) *best_variant = all[0].variant;
+    if (best_max_stages) *best_max_stages = all[0].max_stages;
+    if (best_ms) *best_ms = all[0].ms;
   });
 }
 

@@ -8,10 +8,12 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "host_field.hpp"
 #include "msm.hpp"
+#include "msm_f64.cuh"
 #include "msm_kernels.cuh"
 
 namespace zkg {
@@ -46,6 +48,7 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   half = 1u << (c - 1);
   slots = (size_t)windows * half;
   seg_len = item_points ? item_points : auto_seg_len(n, windows);
+  acc_variant = group == ZKG_G1 ? 4 : 1;
   const size_t xw = xyzz_words();
   const size_t max_entries = (size_t)windows * n;
   if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
@@ -139,7 +142,13 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
-      if (acc_variant == 1)
+      if (acc_variant == 3 && std::is_same<F, Fq>::value)
+        msm_accumulate_f64<true><<<grid_for(heads_max, 128), 128, 0, s>>>(
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      else if (acc_variant == 4 && std::is_same<F, Fq>::value)
+        msm_accumulate_f64<false><<<grid_for(heads_max, 128), 128, 0, s>>>(
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      else if (acc_variant == 1)
         msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
             bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else if (acc_variant == 2)
@@ -150,8 +159,21 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
+    case kStageMerge:
+    case kStageReduce:
+    case kStageWindows:
+    case kStageCombine:
+      // Two products per out-of-line call in every form (measured faster than one per call for
+      // both groups, although the paired Fq2 kernels spill).
+      tail_stage<typename PairedOf<F>::type>(which, s);
+      break;
+  }
+}
+
+template <class FC>
+void MsmPlan::tail_stage(int which, cudaStream_t s) {
+  switch (which) {
     case kStageMerge: {
-      using FC = typename PairedOf<F>::type;
       size_t len = heads_max;
       for (uint32_t l = 0; l < merge_levels; l++) {
         size_t out_len = (len + kMergeFanIn - 1) / kMergeFanIn;
@@ -165,7 +187,6 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       break;
     }
     case kStageReduce: {
-      using FC = typename PairedOf<F>::type;
       const uint32_t* in = buckets.ptr;
       uint32_t in_stride = half;
       for (uint32_t l = 0; l < levels.count; l++) {
@@ -182,14 +203,13 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       break;
     }
     case kStageWindows: {
-      using FC = typename PairedOf<F>::type;
       msm_window_sums<FC><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<FC>), s>>>(tots.ptr, levels,
                                                                                             window_sums.ptr);
       check_launch("msm_window_sums");
       break;
     }
     case kStageCombine:
-      msm_combine<typename PairedOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      msm_combine<FC><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
       check_launch("msm_combine");
       break;
   }

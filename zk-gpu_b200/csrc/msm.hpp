@@ -32,8 +32,11 @@ struct MsmPlan {
   // Accumulation kernel form: 0 = field products inlined, 1 = through one out-of-line product
   // (smaller code: the inlined mixed addition is thousands of instructions and its warps stall
   // on instruction fetch; measured 17% faster at 2^24), 2 = out of line, independent products
-  // two per call (a further 5% at 2^20 and 2^24). Tunable.
-  int acc_variant = 2;
+  // two per call (a further 5% at 2^20 and 2^24 for G1; slower for G2, whose pairs of Fq2
+  // operands no longer fit the argument registers), 3 / 4 = G1 only: bucket arithmetic in
+  // double-precision limbs (msm_f64.cuh), two products per call / one (4: 12% faster than 2
+  // at 2^24). Defaults: 4 for G1, 1 for G2. Tunable.
+  int acc_variant = 4;
   size_t slots = 0, heads_max = 0;
   uint32_t merge_levels = 0, scan_tiles_n = 0;
   ReduceLevels levels;
@@ -58,6 +61,8 @@ struct MsmPlan {
  private:
   template <class F>
   void stage(int which, const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
+  template <class FC>
+  void tail_stage(int which, cudaStream_t s);
 };
 
 }  // namespace zkg

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "field.cuh"
+#include "field_f64.cuh"
 #include "host_field.hpp"
 #include "ntt.hpp"
 
@@ -26,6 +27,10 @@ namespace zkg {
 constexpr uint32_t kTileLog = 11;
 constexpr uint32_t kNttThreads = 256;
 constexpr uint32_t kMaxStagesPerPass = 9;
+// The double-precision form keeps five 8-byte limbs per element in shared memory: tiles of 2^10
+// elements (40 KiB) and passes of at most 8 stages keep the same four-element global runs.
+constexpr uint32_t kTileLogD = 10;
+constexpr uint32_t kMaxStagesPerPassD = 8;
 
 // tw[j] = hi[j >> lo_bits] * lo[j & (2^lo_bits - 1)], j < count (twiddles.wgsl:13-21).
 __global__ void ntt_twiddles(const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint32_t lo_bits,
@@ -96,6 +101,130 @@ __global__ void __launch_bounds__(kNttThreads, 3)
   }
 }
 
+// ------------------------------------------------------------------ double-precision form
+//
+// The same passes with the butterflies in five 52-bit limbs per element (field_f64.cuh;
+// Montgomery products issue on the FP64 pipe). Twiddles are held as limbs in Montgomery form
+// with R = 2^260, so a product x * tw of a plain x still returns x * w^j. Elements stay below 2r
+// in shared memory: x + y is reduced from below 4r, and (x - y + 2r) * tw is below 2r.
+
+__device__ const f64::MultiplesOf<f64::FrLimbs> g_multiples_of_r = f64::MultiplesOf<f64::FrLimbs>();
+
+// Limbs (R = 2^260) of the R = 2^256 Montgomery twiddles, count of them, five doubles each.
+__global__ void ntt_twiddles_to_limbs(const uint32_t* __restrict__ tw, size_t count, double* __restrict__ out) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  const Fr a = load_fe<Fr>(tw + 8 * j);
+  uint32_t w[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) w[i] = a.w[i];
+  const f64::FqD d = f64::fqd_reduce<f64::FrLimbs>(f64::fqd_from_words_x16(w), &g_multiples_of_r);
+#pragma unroll
+  for (int k = 0; k < 5; k++) out[5 * j + k] = d.l[k];
+}
+
+__device__ __forceinline__ f64::FqD tile_load_d(const double* tile, uint32_t elems, uint32_t slot) {
+  return f64::FqD{{tile[slot], tile[elems + slot], tile[2 * elems + slot], tile[3 * elems + slot],
+                   tile[4 * elems + slot]}};
+}
+__device__ __forceinline__ void tile_store_d(double* tile, uint32_t elems, uint32_t slot, const f64::FqD& v) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) tile[k * elems + slot] = v.l[k];
+}
+
+// Canonical words of an element below 2r.
+__device__ __forceinline__ Fr fr_from_limbs(const f64::FqD& v) {
+  uint32_t w[8];
+  f64::limbs_to_words(v.l, w);
+  const uint32_t rw[8] = {FrParams::P0, FrParams::P1, FrParams::P2, FrParams::P3,
+                          FrParams::P4, FrParams::P5, FrParams::P6, FrParams::P7};
+  uint32_t d[8];
+  uint32_t borrow = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint64_t t = (uint64_t)w[i] - rw[i] - borrow;
+    d[i] = (uint32_t)t;
+    borrow = (uint32_t)(t >> 63);
+  }
+  Fr r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.w[i] = borrow ? w[i] : d[i];
+  return r;
+}
+
+// ntt_pass with double-precision butterflies; tw holds 5 doubles per twiddle, the tile is stored
+// limb-major (limb k of slot e at k * elems + e) so consecutive threads touch consecutive doubles.
+template <bool LAST>
+__global__ void __launch_bounds__(kNttThreads, 2)
+    ntt_pass_f64(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const double* __restrict__ tw,
+                 uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale_mont) {
+  using namespace f64;
+  extern __shared__ __align__(16) double tile_d[];
+  const MultiplesOf<FrLimbs>* kr = &g_multiples_of_r;
+  const uint32_t lg = tl - s;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t elems = 1u << tl;
+
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    const uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    const Fr v = load_fe_cg<Fr>(src + 8 * (size_t)g);
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = v.w[i];
+    FqD d;
+    words_to_limbs(w, d.l);
+    tile_store_d(tile_d, elems, slot, d);
+  }
+  __syncthreads();
+
+  const uint32_t t0 = log_n - lm - s;
+  const uint32_t half_elems = elems >> 1;
+  for (uint32_t st = 0; st < s; st++) {
+    const uint32_t lh = s - 1 - st;
+    const uint32_t t = t0 + st;
+    for (uint32_t b = threadIdx.x; b < half_elems; b += kNttThreads) {
+      const uint32_t col = b & ((1u << lg) - 1);
+      const uint32_t q = b >> lg;
+      const uint32_t r_lo = q & ((1u << lh) - 1);
+      const uint32_t row_a = ((q >> lh) << (lh + 1)) + r_lo;
+      const uint32_t slot_a = (row_a << lg) + col;
+      const uint32_t slot_b = slot_a + (1u << (lh + lg));
+      const uint32_t c = (tile << lg) + col;
+      const uint32_t j0 = c & ((1u << lm) - 1);
+      const uint32_t idx = ((r_lo << lm) + j0) << t;
+      const FqD x = tile_load_d(tile_d, elems, slot_a);
+      const FqD y = tile_load_d(tile_d, elems, slot_b);
+      tile_store_d(tile_d, elems, slot_a, fqd_reduce<FrLimbs>(fqd_add(x, y), kr));
+      const FqD d = fqd_sub<2, FrLimbs>(x, y);  // (0, 4r)
+      FqD out;
+      if (idx != 0) {
+        const double* w = tw + 5 * (size_t)idx;
+        const FqD wd{{__ldg(w), __ldg(w + 1), __ldg(w + 2), __ldg(w + 3), __ldg(w + 4)}};
+        out = fqd_mul<FrLimbs>(d, wd);
+      } else {
+        out = fqd_reduce<FrLimbs>(d, kr);
+      }
+      tile_store_d(tile_d, elems, slot_b, out);
+    }
+    __syncthreads();
+  }
+
+  FqD scale;
+  if (scale_flag) {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = scale_mont.w[i];
+    scale = fqd_reduce<FrLimbs>(fqd_from_words_x16(w), kr);
+  }
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    FqD v = tile_load_d(tile_d, elems, slot);
+    if (scale_flag) v = fqd_mul<FrLimbs>(v, scale);
+    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    if (LAST) g = __brev(g) >> (32 - log_n);
+    store_fe(dst + 8 * (size_t)g, fr_from_limbs(v));
+  }
+}
+
 static std::vector<uint32_t> powers_words(const host::U256& step, size_t len) {
   const host::Field& f = host::fr();
   std::vector<uint32_t> out(8 * len);
@@ -121,21 +250,46 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   scratch.alloc(8 * n, "ntt scratch");
   build_twiddles(w, fwd_tw);
   build_twiddles(w_inv, inv_tw);
-
-  // Pass split: one tile when it fits, else ceil(log_n / 9) passes of near-equal size.
-  set_max_stages(kMaxStagesPerPass);
   const size_t smem = (size_t)32 << (log_n < kTileLog ? log_n : kTileLog);
   check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
   check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
+  set_variant(0);
+}
+
+uint32_t NttPlan::tile_log() const { return variant == 1 ? kTileLogD : kTileLog; }
+
+bool NttPlan::set_variant(int v) {
+  if (v != 0 && v != 1) return false;
+  if (v == 1 && !fwd_twd.ptr) {  // twiddle limbs on first use of the double-precision form
+    const size_t count = (size_t)1 << (log_n - 1);
+    use(ctx);
+    fwd_twd.alloc(10 * count, "ntt twiddle limbs");
+    inv_twd.alloc(10 * count, "ntt twiddle limbs");
+    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->stream>>>(fwd_tw.ptr, count,
+                                                                        reinterpret_cast<double*>(fwd_twd.ptr));
+    check_launch("ntt_twiddles_to_limbs");
+    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->stream>>>(inv_tw.ptr, count,
+                                                                        reinterpret_cast<double*>(inv_twd.ptr));
+    check_launch("ntt_twiddles_to_limbs");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "ntt twiddle limbs");  // enqueue may use another stream
+  }
+  variant = v;
+  // Pass split: one tile when it fits, else passes of near-equal size, at most 9 stages each
+  // (integer form, tiles of 2^11) or 8 (double-precision form, tiles of 2^10).
+  set_max_stages(v == 1 ? kMaxStagesPerPassD : kMaxStagesPerPass);
+  return true;
 }
 
 bool NttPlan::set_max_stages(uint32_t ms) {
-  if (ms < 6 || ms > kTileLog) return false;
-  if (log_n <= kTileLog) {
+  const uint32_t tlog = tile_log();
+  const uint32_t def = variant == 1 ? kMaxStagesPerPassD : kMaxStagesPerPass;
+  if (ms < 6 || ms > tlog) return false;
+  if (log_n <= tlog) {
     passes.assign(1, log_n);
-    return ms == kMaxStagesPerPass;
+    max_stages = def;
+    return ms == def;
   }
   max_stages = ms;
   uint32_t p = (log_n + ms - 1) / ms;
@@ -167,11 +321,13 @@ void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out) {
 
 void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
   const uint32_t* tw = inverse ? inv_tw.ptr : fwd_tw.ptr;
+  const double* twd = reinterpret_cast<const double*>(inverse ? inv_twd.ptr : fwd_twd.ptr);
   Fr scale;
   std::memcpy(scale.w, n_inv_words, sizeof(scale.w));
-  const uint32_t tl = log_n < kTileLog ? log_n : kTileLog;
+  const uint32_t tlog = tile_log();
+  const uint32_t tl = log_n < tlog ? log_n : tlog;
   const unsigned tiles = 1u << (log_n - tl);
-  const size_t smem = (size_t)32 << tl;
+  const size_t smem = variant == 1 ? (size_t)40 << tl : (size_t)32 << tl;
   uint32_t done = 0;
   const size_t np = passes.size();
   for (size_t i = 0; i < np; i++) {
@@ -182,7 +338,11 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
     uint32_t* dst = last ? data : scratch.ptr;
     const int scale_flag = last && inverse;
     size_t ev = timer.enabled ? timer.begin((int)i, s) : 0;
-    if (last)
+    if (variant == 1 && last)
+      ntt_pass_f64<true><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale);
+    else if (variant == 1)
+      ntt_pass_f64<false><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale);
+    else if (last)
       ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
     else
       ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);

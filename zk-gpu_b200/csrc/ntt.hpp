@@ -12,11 +12,18 @@ struct NttPlan {
   uint32_t log_n;
   std::vector<uint32_t> passes;  // stages per pass
   uint32_t n_inv_words[8];       // 1/n in Montgomery form
-  DeviceArray scratch, fwd_tw, inv_tw;
+  // twiddles w^j, j < n/2: 8 words (R = 2^256) and five double limbs (R = 2^260) each
+  DeviceArray scratch, fwd_tw, inv_tw, fwd_twd, inv_twd;
   StageTimer timer;  // one stage id per pass
 
   NttPlan(zkg_ctx* ctx, uint32_t log_n);
-  // Splits the stages into passes of at most max_stages (6..11); false if not applicable
+  // Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs (measured
+  // 12% slower at 2^24 on B200; the tuner may still pick it). Resets the pass split to the
+  // form's default. The first switch to form 1 builds its twiddle limbs on the plan's stream.
+  bool set_variant(int variant);
+  int variant = 0;
+  uint32_t tile_log() const;
+  // Splits the stages into passes of at most max_stages (6..tile_log()); false if not applicable
   // (transforms of one tile have a single pass).
   bool set_max_stages(uint32_t max_stages);
   uint32_t max_stages = 9;

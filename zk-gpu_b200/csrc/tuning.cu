@@ -54,7 +54,10 @@ std::vector<zkg_msm_tuning> tune_msm(zkg_ctx* ctx, int group, size_t n, const zk
         throw;
       }
       plan->check_buffers(bases, scalars);
-      for (int v = 0; v <= 2; v++) {
+      // forms that can win: out-of-line integer products (1, 2) and, for G1, double-precision
+      // limbs (3, 4); fully inlined products (0) lose to both everywhere measured
+      const std::vector<int> variants = group == ZKG_G1 ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{1, 2};
+      for (int v : variants) {
         plan->acc_variant = v;
         double ms = time_ms(ctx->stream, reps, [&] { plan->enqueue(bases->ptr, scalars->ptr, ctx->stream); });
         out.push_back(zkg_msm_tuning{(uint32_t)c, L, v, ms});
@@ -65,20 +68,25 @@ std::vector<zkg_msm_tuning> tune_msm(zkg_ctx* ctx, int group, size_t n, const zk
   return out;
 }
 
-std::vector<std::pair<uint32_t, double>> tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps) {
+std::vector<NttChoice> tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps) {
   use(ctx);
   std::unique_ptr<NttPlan> plan(new NttPlan(ctx, log_n));
   if (data->words < ((size_t)8 << log_n)) fail(ZKG_ESIZE, "data buffer too small for the transform");
-  std::vector<std::pair<uint32_t, double>> out;
-  for (uint32_t s = 6; s <= 11; s++) {
-    if (!plan->set_max_stages(s)) continue;
-    double ms = time_ms(ctx->stream, reps, [&] {
-      plan->enqueue(data->ptr, false, ctx->stream);
-      plan->enqueue(data->ptr, true, ctx->stream);
-    });
-    out.push_back({s, ms / 2});
+  std::vector<NttChoice> out;
+  for (int v = 0; v <= 1; v++) {
+    plan->set_variant(v);
+    const uint32_t tlog = plan->tile_log();
+    for (uint32_t s = 6; s <= tlog; s++) {
+      if (!plan->set_max_stages(s)) continue;
+      if (plan->passes.size() == 1 && s != tlog) continue;  // one tile: every split is the same
+      double ms = time_ms(ctx->stream, reps, [&] {
+        plan->enqueue(data->ptr, false, ctx->stream);
+        plan->enqueue(data->ptr, true, ctx->stream);
+      });
+      out.push_back(NttChoice{v, s, ms / 2});
+    }
   }
-  std::sort(out.begin(), out.end(), [](auto& a, auto& b) { return a.second < b.second; });
+  std::sort(out.begin(), out.end(), [](const NttChoice& a, const NttChoice& b) { return a.ms < b.ms; });
   return out;
 }
 

@@ -98,9 +98,12 @@ SIGNATURES = {
     "zkg_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
     "zkg_tune_msm": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_size_t, vp, vp, ctypes.c_int,
                                     ctypes.POINTER(MsmTuning), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "zkg_ntt_set_variant": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_ntt_set_max_stages": (ctypes.c_int, [vp, ctypes.c_uint32]),
-    "zkg_tune_ntt": (ctypes.c_int, [vp, ctypes.c_uint32, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32),
-                                    ctypes.POINTER(ctypes.c_double)]),
+    "zkg_ntt_params": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint32)]),
+    "zkg_tune_ntt": (ctypes.c_int, [vp, ctypes.c_uint32, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double)]),
     "zkg_ntt_noalloc": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, vp, vp]),
     "zkg_ctx_stream": (vp, [vp]),
     "zkg_launch_count": (ctypes.c_uint64, []),

@@ -67,13 +67,15 @@ def tuned_msm(gpu: Gpu, group: Group, n: int, bases: Buffer, scalars: Buffer, re
 
 
 def tuned_ntt(gpu: Gpu, log_n: int, data: Buffer, reps: int = 2, refresh: bool = False) -> Ntt:
-    key = f"{gpu.adapter_name}|ntt|{log_n}"
+    key = f"{gpu.adapter_name}|ntt2|{log_n}"
     cache = _load()
     if refresh or key not in cache:
-        best, ms = ctypes.c_uint32(), ctypes.c_double()
-        check(lib().zkg_tune_ntt(gpu.handle, log_n, data.handle, reps, ctypes.byref(best), ctypes.byref(ms)))
-        cache[key] = {"max_stages": best.value, "ms": ms.value}
+        var, best, ms = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
+        check(lib().zkg_tune_ntt(gpu.handle, log_n, data.handle, reps, ctypes.byref(var), ctypes.byref(best),
+                                 ctypes.byref(ms)))
+        cache[key] = {"variant": var.value, "max_stages": best.value, "ms": ms.value}
         _store(cache)
     ntt = Ntt(gpu, log_n)
+    ntt.set_variant(cache[key]["variant"])
     check(lib().zkg_ntt_set_max_stages(ntt.handle, cache[key]["max_stages"]))
     return ntt

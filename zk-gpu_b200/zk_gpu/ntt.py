@@ -37,6 +37,18 @@ class Ntt:
         """In-place inverse transform, including the 1/n factor."""
         check(lib().zkg_ntt_inverse(self._h, data.handle))
 
+    def set_variant(self, variant: int) -> None:
+        """Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs."""
+        check(lib().zkg_ntt_set_variant(self._h, variant))
+
+    def set_max_stages(self, max_stages: int) -> None:
+        check(lib().zkg_ntt_set_max_stages(self._h, max_stages))
+
+    def params(self) -> dict:
+        v, ms, p = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().zkg_ntt_params(self._h, ctypes.byref(v), ctypes.byref(ms), ctypes.byref(p)))
+        return {"variant": v.value, "max_stages": ms.value, "passes": p.value}
+
     def close(self) -> None:
         if self._h:
             lib().zkg_ntt_free(self._h)
