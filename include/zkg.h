@@ -110,6 +110,11 @@ int zkg_msm_group(const zkg_msm *msm);
  * for G2). Defaults: 4 for G1, 1 for G2.
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
+/* Counting-sort knob (no reference counterpart): how a warp merges the counting pass's atomics
+ * for lanes whose digits hit the same (window, bucket) slot: 0 = every group of equal slots
+ * (default), 1 = the group of the first lane only, 2 = none, 3 = the group of the first pair of
+ * neighbouring lanes with equal slots. The scatter pass always merges every group. */
+int zkg_msm_set_sort(zkg_msm *msm, int mode);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,
@@ -308,7 +313,8 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
  * (FMAs counted); 15 / 16 / 17 = the double-precision product with the product-phase column adds,
  * every column add, or the low halves' adds issued as integer multiply-adds by 1; 18 / 19 = one
  * dependent chain of Fq products on a single thread (integer / double-precision form; products
- * per second = 1 / latency);
+ * per second = 1 / latency); 20 / 21 / 22 = a chain of XYZZ doublings on one thread with inlined
+ * products / one out-of-line product per call / two per call (doublings per second);
  * alternative forms are first checked on the device against the production product.
  * *ops_per_second receives multiply-adds (or products, or FMAs) per second on the context's
  * device; the best of five launches over every SM. */

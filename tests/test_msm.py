@@ -329,3 +329,20 @@ def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
     assert msm.params() == again.params()
     got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, bb, sb), 32)))
     assert np.array_equal(got, msm_ref("G1", bases, s))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_sort_aggregation_modes_agree(gpu, mode):
+    """The counting sort's warp aggregation modes (every group / first lane's group / none) on
+    inputs that put many lanes of a warp into one slot and on uniform ones."""
+    n, c = 20000, 12
+    bases = random_points("G1", 960, n)
+    cases = [("uniform", scalar_distribution(n, "uniform", 961)), ("sparse", scalar_distribution(n, "sparse", 962)),
+             ("r-1", scalar_distribution(n, "r-1", 963)), ("all ones", fr_words([1] * n)),
+             ("alternating", fr_words([5 if i % 2 else R - 5 for i in range(n)]))]
+    for name, s in cases:
+        for items in (None, 3):
+            msm = Msm.with_item_points(gpu, n, c, items) if items else Msm(gpu, n, c)
+            msm.set_sort(mode)
+            got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, Msm.upload_bases(gpu, bases), gpu.buffer(s)), 32)))
+            assert np.array_equal(got, msm_ref("G1", bases, s)), (name, items, mode)

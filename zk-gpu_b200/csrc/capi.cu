@@ -253,6 +253,14 @@ int zkg_msm_set_variant(zkg_msm* msm, int variant) {
   });
 }
 
+int zkg_msm_set_sort(zkg_msm* msm, int mode) {
+  return guard([&] {
+    need(msm, "msm");
+    if (mode < 0 || mode > 3) fail(ZKG_EINVAL, "sort aggregation mode must be 0..3");
+    msm->plan.sort_agg = mode;
+  });
+}
+
 int zkg_msm_params(const zkg_msm* msm, uint32_t* c, uint32_t* item_points, int* variant) {
   return guard([&] {
     need(msm, "msm");
@@ -451,7 +459,7 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 19) fail(ZKG_EINVAL, "variant must be 0..19");
+    if (variant < 0 || variant > 22) fail(ZKG_EINVAL, "variant must be 0..22");
     *ops_per_second = bench_integer_pipe(ctx, variant);
   });
 }

@@ -126,7 +126,14 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
   switch (which) {
     case kStageCount:
       check_cuda(cudaMemsetAsync(counts.ptr, 0, slots * 4, s), "msm counts clear");
-      msm_count<<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+      if (sort_agg == 1)
+        msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+      else if (sort_agg == 2)
+        msm_count<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+      else if (sort_agg == 3)
+        msm_count<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+      else
+        msm_count<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
       check_launch("msm_count");
       break;
     case kStageScan:
@@ -138,7 +145,8 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("scan_apply");
       break;
     case kStageScatter:
-      msm_scatter<<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
+      // every group merged: measured best or equal for the scatter on every distribution
+      msm_scatter<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
@@ -159,10 +167,15 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
+    case kStageCombine:
+      // c (W - 1) dependent doublings: one warp, each level's independent products on separate
+      // lanes (one out-of-line product per lane).
+      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      check_launch("msm_combine_lanes");
+      break;
     case kStageMerge:
     case kStageReduce:
     case kStageWindows:
-    case kStageCombine:
       // Two products per out-of-line call in every form (measured faster than one per call for
       // both groups, although the paired Fq2 kernels spill).
       tail_stage<typename PairedOf<F>::type>(which, s);
@@ -208,9 +221,7 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
       check_launch("msm_window_sums");
       break;
     }
-    case kStageCombine:
-      msm_combine<FC><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
-      check_launch("msm_combine");
+    case kStageCombine:  // launched by stage() (msm_combine_lanes)
       break;
   }
 }

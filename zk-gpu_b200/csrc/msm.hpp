@@ -37,6 +37,10 @@ struct MsmPlan {
   // double-precision limbs (msm_f64.cuh), two products per call / one (4: 12% faster than 2
   // at 2^24). Defaults: 4 for G1, 1 for G2. Tunable.
   int acc_variant = 4;
+  // Warp aggregation of the counting pass's atomics (slot_peers in msm_kernels.cuh): 0 = every
+  // group of equal slots, 1 = the first lane's group, 2 = none, 3 = the group of the first equal
+  // neighbour pair. The scatter pass always merges every group.
+  int sort_agg = 3;
   size_t slots = 0, heads_max = 0;
   uint32_t merge_levels = 0, scan_tiles_n = 0;
   ReduceLevels levels;

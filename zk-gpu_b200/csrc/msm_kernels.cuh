@@ -29,6 +29,7 @@
 //   8. combine          Horner over windows, c doublings each      [msm_combine.wgsl]
 #pragma once
 #include "curve.cuh"
+#include "curve_lanes.cuh"
 #include "msm_common.hpp"
 
 namespace zkg {
@@ -78,8 +79,46 @@ struct Recoder {
   }
 };
 
-// Pass 1: histogram of (window, bucket) slots. Lanes of a warp that hit the same slot are
-// merged into one atomic (equal scalars, zero-heavy or r-1-heavy inputs hammer single slots).
+// Lanes of a warp that share a slot, for one atomic per group. AGG 0: every group
+// (__match_any_sync); 1: only the group of the first lane that has a slot (one shuffle and one
+// ballot: skewed inputs put most repeats into one hot slot per window); 2: none; 3: the group of
+// the first lane whose right neighbour has the same slot (a slot held by a sizeable share of
+// the warp almost always shows up in an adjacent pair; uniform digits almost never do, and
+// then no group forms). Lanes without a slot (kNoKey) get an empty mask.
+template <int AGG>
+__device__ __forceinline__ unsigned slot_peers(uint32_t slot) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned active = __activemask();
+  if (AGG == 0) {
+    const unsigned m = __match_any_sync(active, slot);  // every lane of the mask takes part
+    return slot == kNoKey ? 0u : m;
+  }
+  if (AGG == 1) {
+    const unsigned valid = __ballot_sync(active, slot != kNoKey);
+    if (!valid) return 0u;
+    const int first = __ffs(valid) - 1;
+    const uint32_t hot = __shfl_sync(active, slot, first);
+    const unsigned group = __ballot_sync(active, slot == hot) & valid;
+    if (slot == kNoKey) return 0u;
+    return slot == hot ? group : (1u << lane);
+  }
+  if (AGG == 3) {
+    const unsigned valid = __ballot_sync(active, slot != kNoKey);
+    const uint32_t right = __shfl_down_sync(active, slot, 1);
+    const unsigned pairs = __ballot_sync(active, slot != kNoKey && lane < 31 && slot == right);
+    if (slot == kNoKey) return 0u;
+    if (!pairs) return 1u << lane;
+    const uint32_t hot = __shfl_sync(valid | pairs, slot, __ffs(pairs) - 1);
+    const unsigned group = __ballot_sync(valid, slot == hot);
+    return slot == hot ? group : (1u << lane);
+  }
+  return slot == kNoKey ? 0u : (1u << lane);
+}
+
+// Pass 1: histogram of (window, bucket) slots; lanes of a warp that hit the same slot are
+// merged into one atomic as slot_peers<AGG> groups them (equal scalars, zero-heavy or
+// r-1-heavy inputs hammer single slots).
+template <int AGG>
 __global__ void msm_count(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
                           uint32_t* __restrict__ counts) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -87,20 +126,18 @@ __global__ void msm_count(const uint32_t* __restrict__ scalars, size_t n, uint32
   Recoder rc;
   if (live) load_scalar(scalars, i, rc.s);
   uint32_t half = 1u << (c - 1);
+  const unsigned lane = threadIdx.x & 31;
   for (uint32_t w = 0; w < windows; w++) {
     bool neg;
     uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
-    unsigned active = __activemask();
-    unsigned peers = __match_any_sync(active, slot);
-    if (slot != kNoKey) {
-      int leader = __ffs(peers) - 1;
-      if ((int)(threadIdx.x & 31) == leader) atomicAdd(&counts[slot], (uint32_t)__popc(peers));
-    }
+    const unsigned peers = slot_peers<AGG>(slot);
+    if (peers && (int)lane == __ffs(peers) - 1) atomicAdd(&counts[slot], (uint32_t)__popc(peers));
   }
 }
 
 // Pass 3: scatter point indices (sign in bit 31) into slot order. Within a slot the order is
 // whatever the atomics give; bucket sums are exact, so the result does not depend on it.
+template <int AGG>
 __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
                             uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -108,20 +145,21 @@ __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint
   Recoder rc;
   if (live) load_scalar(scalars, i, rc.s);
   uint32_t half = 1u << (c - 1);
-  unsigned lane = threadIdx.x & 31;
+  const unsigned lane = threadIdx.x & 31;
   for (uint32_t w = 0; w < windows; w++) {
     bool neg = false;
     uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
-    unsigned active = __activemask();
-    unsigned peers = __match_any_sync(active, slot);
-    if (slot != kNoKey) {
-      int leader = __ffs(peers) - 1;
-      uint32_t base = 0;
-      if ((int)lane == leader) base = atomicAdd(&cursor[slot], (uint32_t)__popc(peers));
-      base = __shfl_sync(peers, base, leader);
-      uint32_t rank = __popc(peers & ((1u << lane) - 1));
-      sorted[base + rank] = (uint32_t)i | (neg ? kNegBit : 0u);
+    const unsigned peers = slot_peers<AGG>(slot);
+    if (AGG == 2) {
+      if (peers) sorted[atomicAdd(&cursor[slot], 1u)] = (uint32_t)i | (neg ? kNegBit : 0u);
+      continue;
     }
+    // every lane takes part in the shuffle below: groups are disjoint, each with its own leader
+    const int leader = peers ? __ffs(peers) - 1 : (int)lane;
+    uint32_t base = 0;
+    if (peers && (int)lane == leader) base = atomicAdd(&cursor[slot], (uint32_t)__popc(peers));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (peers) sorted[base + __popc(peers & ((1u << lane) - 1))] = (uint32_t)i | (neg ? kNegBit : 0u);
   }
 }
 
@@ -394,13 +432,15 @@ __device__ Xyzz<F> block_sum(Xyzz<F> v, Xyzz<F>* sh) {
 }
 
 // One block per window: S_w = sum over levels l of 16^l * sum_k tot_l[k], folded from the top
-// level down (4 doublings per level).
+// level down (4 doublings per level) by warp 0 with lane-parallel products.
 template <class F>
 __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t* __restrict__ tots, ReduceLevels lv,
                                                                   uint32_t* __restrict__ window_sums) {
   constexpr int XW = PointWords<F>::xyzz;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Xyzz<F>* sh = reinterpret_cast<Xyzz<F>*>(smem_raw);
+  __shared__ uint32_t scratch[32 * 8];
+  const LaneScratch sm{scratch};
   const uint32_t w = blockIdx.x;
   Xyzz<F> acc = xyzz_infinity<F>();
   for (int l = (int)lv.count - 1; l >= 0; l--) {
@@ -408,26 +448,29 @@ __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t
     const uint32_t* base = tots + ((size_t)lv.tot_offset[l] + (size_t)w * lv.tot_len[l]) * XW;
     for (uint32_t k = threadIdx.x; k < lv.tot_len[l]; k += blockDim.x) part = xyzz_add(part, load_xyzz<F>(base + (size_t)k * XW));
     part = block_sum(part, sh);
-    if (threadIdx.x == 0) {
-      for (int d = 0; d < 4; d++) acc = xyzz_double(acc);  // x16 = kChunk
-      acc = xyzz_add(acc, part);
+    if (threadIdx.x < 32) {  // warp 0 folds the levels, products of a level on separate lanes
+      for (int d = 0; d < 4; d++) acc = lane_double(acc, sm);  // x16 = kChunk
+      acc = lane_add(acc, part, sm);
     }
   }
   if (threadIdx.x == 0) store_xyzz(window_sums + (size_t)w * XW, acc);
 }
 
-// result = sum_w 2^(c*w) S_w by Horner from the top window (msm_combine.wgsl:13-22).
+// result = sum_w 2^(c*w) S_w by Horner from the top window (msm_combine.wgsl:13-22), by one
+// warp: each level's independent products run on separate lanes (curve_lanes.cuh). F is the
+// one-product-per-call form (FqC or Fq2C).
 template <class F>
-__global__ void msm_combine(const uint32_t* __restrict__ window_sums, uint32_t windows, uint32_t c,
-                            uint32_t* __restrict__ result) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(32) msm_combine_lanes(const uint32_t* __restrict__ window_sums, uint32_t windows,
+                                                        uint32_t c, uint32_t* __restrict__ result) {
+  __shared__ uint32_t scratch[32 * 8];
+  const LaneScratch sm{scratch};
   constexpr int XW = PointWords<F>::xyzz;
   Xyzz<F> acc = load_xyzz<F>(window_sums + (size_t)(windows - 1) * XW);
   for (int w = (int)windows - 2; w >= 0; w--) {
-    for (uint32_t k = 0; k < c; k++) acc = xyzz_double(acc);
-    acc = xyzz_add(acc, load_xyzz<F>(window_sums + (size_t)w * XW));
+    for (uint32_t k = 0; k < c; k++) acc = lane_double(acc, sm);
+    acc = lane_add(acc, load_xyzz<F>(window_sums + (size_t)w * XW), sm);
   }
-  store_xyzz(result, acc);
+  if (threadIdx.x == 0) store_xyzz(result, acc);
 }
 
 // ------------------------------------------------------------------ base upload

@@ -394,6 +394,17 @@ __global__ void mulmod_latency_kernel(uint32_t* out, uint32_t iters, uint32_t se
   }
 }
 
+// A chain of XYZZ doublings on one thread (the combine stage's critical path), in a given
+// product form: variants 20 (inlined), 21 (one out-of-line product per call), 22 (pairs).
+template <class F>
+__global__ void doubling_chain_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
+  Xyzz<F> p{F::one(), F::one(), F::one(), F::one()};
+  p.x.w[0] ^= seed;
+  p.y.w[1] ^= seed * 7u;
+  for (uint32_t it = 0; it < iters; it++) p = xyzz_double(p);
+  if (p.x.w[0] == 0x9e3779b9u) out[0] = p.y.w[0];
+}
+
 // 16 a mod p for a canonical Fq value: the factor between Montgomery forms with R = 2^256 and
 // R = 2^260 of the same element.
 __device__ __forceinline__ Fq times16(Fq a) {
@@ -447,6 +458,28 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   sink.alloc(16, "sink");
   const unsigned blocks = (unsigned)ctx->sm_count * 8, threads = 256;
   const bool product = variant == 3 || (variant >= 6 && variant <= 8) || variant == 11 || variant == 12 || variant >= 15;
+  if (variant >= 20 && variant <= 22) {  // doublings per second on one thread
+    const uint32_t chain = 2048;
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    auto go = [&](uint32_t iters) {
+      if (variant == 20) doubling_chain_kernel<Fq><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
+      if (variant == 21) doubling_chain_kernel<FqC><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
+      if (variant == 22) doubling_chain_kernel<FqCP><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
+      check_launch("doubling_chain_kernel");
+    };
+    go(16);
+    check_cuda(cudaEventRecord(e0, ctx->stream), "event");
+    go(chain);
+    check_cuda(cudaEventRecord(e1, ctx->stream), "event");
+    check_cuda(cudaEventSynchronize(e1), "doubling probe");
+    float ms = 0;
+    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return chain / (ms * 1e-3);
+  }
   if (variant == 18 || variant == 19) {  // single-thread latency: products per second of one chain
     const uint32_t chain = 20000;
     cudaEvent_t e0, e1;

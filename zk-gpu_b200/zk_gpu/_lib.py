@@ -66,6 +66,7 @@ SIGNATURES = {
     "zkg_msm_free": (None, [vp]),
     "zkg_msm_group": (ctypes.c_int, [vp]),
     "zkg_msm_set_variant": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_set_sort": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_msm_params": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_int)]),
     "zkg_msm_run": (ctypes.c_int, [vp, vp, vp, ctypes.POINTER(vp)]),

@@ -66,6 +66,11 @@ class Msm:
         per call. Defaults: 4 for G1, 1 for G2."""
         check(lib().zkg_msm_set_variant(self._h, variant))
 
+    def set_sort(self, mode: int) -> None:
+        """Counting-pass warp aggregation: 0 every group of equal slots, 1 the first lane's
+        group, 2 none, 3 the first equal neighbour pair's group."""
+        check(lib().zkg_msm_set_sort(self._h, mode))
+
     def params(self) -> dict:
         c, items, var = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
         check(lib().zkg_msm_params(self._h, ctypes.byref(c), ctypes.byref(items), ctypes.byref(var)))
