@@ -11,8 +11,8 @@
 // of 2^52 below 2^104), so only the high-half FMA depends on the rounding mode.
 //
 // Reduction: five digit steps in base 2^52, q_i = (t_i mod 2^52) * (-p^-1) mod 2^52; the low half
-// of q_i * p_0 is never formed because t_i + lo(q_i p_0) is the next multiple of 2^52, so the
-// carry into column i+1 is (t_i >> 52) + (t_i mod 2^52 != 0). Inputs below 2p give an output
+// of q_i * p_0 is never formed because t_i + lo(q_i p_0) is the next multiple of 2^52 at or
+// above t_i, so the carry into column i+1 is ceil(t_i / 2^52). Inputs below 2p give an output
 // below 2p (p < 2^254, R = 2^260), so values stay in [0, 2p) between products.
 #pragma once
 #include <cstdint>
@@ -95,9 +95,9 @@ __device__ __forceinline__ void mont_mul(const double (&x)[5], const double (&y)
 #pragma unroll
   for (int i = 0; i < 5; i++) {
     const uint64_t t = c[i];
-    const uint64_t tl = t & kM52;
-    const uint64_t carry = (t >> 52) + (tl != 0 ? 1ull : 0ull);
-    const double tf = limb_to_double(tl);
+    // t + lo(q p_0) is the next multiple of 2^52 at or above t: carry = ceil(t / 2^52)
+    const uint64_t carry = (t + kM52) >> 52;
+    const double tf = limb_to_double(t & kM52);
     const double qh = __fma_rz(tf, (double)L::PINV, kC104);
     const double ql = __fma_rn(tf, (double)L::PINV, __dsub_rn(kC104p52, qh));
     const double q = __dsub_rn(ql, kC52);

@@ -42,7 +42,7 @@ struct MsmPlan {
   // neighbour pair. The scatter pass always merges every group.
   int sort_agg = 3;
   size_t slots = 0, heads_max = 0;
-  uint32_t merge_levels = 0, scan_tiles_n = 0;
+  uint32_t merge_levels = 0, merge_fan_in = 16, scan_tiles_n = 0;
   ReduceLevels levels;
   std::vector<uint32_t> level_m;
 

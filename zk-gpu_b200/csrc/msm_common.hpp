@@ -7,16 +7,17 @@ namespace zkg {
 
 constexpr uint32_t kNegBit = 0x80000000u;
 constexpr uint32_t kNoKey = 0xffffffffu;
-constexpr uint32_t kMergeFanIn = 16;  // heads summed per thread per merge level
-constexpr uint32_t kChunk = 16;       // buckets per running-sum thread
+// Heads summed per thread per merge level, and buckets per running-sum thread (2^chunk_log),
+// chosen per plan: long chains suit many threads, short ones few (MsmPlan).
 constexpr int kScanBlock = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanBlock * kScanItems;
 constexpr int kWindowThreads = 128;
-constexpr int kMaxReduceLevels = 8;
+constexpr int kMaxReduceLevels = 16;
 
 struct ReduceLevels {
   uint32_t count;                         // levels
+  uint32_t chunk_log;                     // buckets per running-sum thread = 2^chunk_log
   uint32_t tot_len[kMaxReduceLevels];     // tot values per window at each level
   uint32_t tot_offset[kMaxReduceLevels];  // start (in points) of level l's tot array; window stride = tot_len
 };

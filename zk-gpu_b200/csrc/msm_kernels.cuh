@@ -331,9 +331,9 @@ __global__ void __launch_bounds__(128) msm_accumulate(const uint32_t* __restrict
 // ------------------------------------------------------------------ merge levels
 
 // Length of the head array at merge level `level` (level 0 = the accumulate output).
-__device__ __forceinline__ uint32_t heads_len(uint32_t total, uint32_t seg_len, uint32_t level) {
+__device__ __forceinline__ uint32_t heads_len(uint32_t total, uint32_t seg_len, uint32_t fan_in, uint32_t level) {
   uint64_t len = ((uint64_t)total + seg_len - 1) / seg_len;
-  for (uint32_t l = 0; l < level; l++) len = (len + kMergeFanIn - 1) / kMergeFanIn;
+  for (uint32_t l = 0; l < level; l++) len = (len + fan_in - 1) / fan_in;
   return (uint32_t)len;
 }
 
@@ -344,23 +344,23 @@ __device__ __forceinline__ void add_into_bucket(uint32_t* buckets, uint32_t key,
   store_xyzz(b, xyzz_add(load_xyzz<F>(b), v));
 }
 
-// Thread u sums heads [u*L1, u*L1 + L1) of level `level`. Runs that start inside the range
-// are added into their bucket; a run that continues from the previous range becomes this
+// Thread u sums heads [u*f, u*f + f) of level `level` (f = fan_in). Runs that start inside the
+// range are added into their bucket; a run that continues from the previous range becomes this
 // thread's head for the next level.
 template <class F>
 __global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ slot_start, uint32_t num_slots,
-                                                 uint32_t seg_len, uint32_t level,
+                                                 uint32_t seg_len, uint32_t fan_in, uint32_t level,
                                                  const uint32_t* __restrict__ in_pts,
                                                  const uint32_t* __restrict__ in_keys, uint32_t* __restrict__ out_pts,
                                                  uint32_t* __restrict__ out_keys, uint32_t* __restrict__ buckets) {
   constexpr int XW = PointWords<F>::xyzz;
   const uint32_t total = __ldg(&slot_start[num_slots]);
-  const uint32_t len = heads_len(total, seg_len, level);
+  const uint32_t len = heads_len(total, seg_len, fan_in, level);
   if (len <= 1) return;  // nothing left to merge
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t q0_64 = (uint64_t)u * kMergeFanIn;
+  const uint64_t q0_64 = (uint64_t)u * fan_in;
   if (q0_64 >= len) return;
-  const uint32_t q0 = (uint32_t)q0_64, q1 = min(q0 + kMergeFanIn, len);
+  const uint32_t q0 = (uint32_t)q0_64, q1 = min(q0 + fan_in, len);
   const uint32_t prev = q0 > 0 ? in_keys[q0 - 1] : kNoKey;
 
   uint32_t cur = kNoKey, start = q0, out_key = kNoKey;
@@ -390,21 +390,22 @@ __global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ sl
 
 // Level of the running-sum reduction. Per window w the input holds m values A_0..A_{m-1} at
 // in + (w * in_stride + b) * XW; level 0 reads the buckets, where an empty slot (no entries)
-// is the point at infinity. Thread (w, k) covers b in [16k, 16k + 16):
-//   tot_k = sum_j (j+1) A_{16k+j}   -> tot_out[w * tot_stride + k]
-//   run_k = sum_j A_{16k+j}          -> run_out[w * run_stride + k - 1]  (k >= 1)
+// is the point at infinity. With chunk C = 2^chunk_log, thread (w, k) covers b in [Ck, Ck + C):
+//   tot_k = sum_j (j+1) A_{Ck+j}   -> tot_out[w * tot_stride + k]
+//   run_k = sum_j A_{Ck+j}          -> run_out[w * run_stride + k - 1]  (k >= 1)
 template <class F>
 __global__ void __launch_bounds__(128) msm_reduce_level(const uint32_t* __restrict__ in, uint32_t in_stride,
-                                                        uint32_t m, uint32_t windows,
+                                                        uint32_t m, uint32_t windows, uint32_t chunk_log,
                                                         const uint32_t* __restrict__ slot_start,
                                                         uint32_t* __restrict__ tot_out, uint32_t tot_stride,
                                                         uint32_t* __restrict__ run_out, uint32_t run_stride) {
   constexpr int XW = PointWords<F>::xyzz;
-  const uint32_t chunks = (m + kChunk - 1) / kChunk;
+  const uint32_t chunk = 1u << chunk_log;
+  const uint32_t chunks = (m + chunk - 1) / chunk;
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= chunks * windows) return;
   const uint32_t w = id / chunks, k = id % chunks;
-  const uint32_t lo = k * kChunk, hi = min(lo + kChunk, m);
+  const uint32_t lo = k * chunk, hi = min(lo + chunk, m);
   Xyzz<F> run = xyzz_infinity<F>(), tot = xyzz_infinity<F>();
   for (uint32_t b = hi; b-- > lo;) {
     size_t slot = (size_t)w * in_stride + b;
@@ -431,8 +432,9 @@ __device__ Xyzz<F> block_sum(Xyzz<F> v, Xyzz<F>* sh) {
   return r;
 }
 
-// One block per window: S_w = sum over levels l of 16^l * sum_k tot_l[k], folded from the top
-// level down (4 doublings per level) by warp 0 with lane-parallel products.
+// One block per window: S_w = sum over levels l of C^l * sum_k tot_l[k] (C = 2^chunk_log),
+// folded from the top level down (chunk_log doublings per level) by warp 0 with lane-parallel
+// products.
 template <class F>
 __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t* __restrict__ tots, ReduceLevels lv,
                                                                   uint32_t* __restrict__ window_sums) {
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t
     for (uint32_t k = threadIdx.x; k < lv.tot_len[l]; k += blockDim.x) part = xyzz_add(part, load_xyzz<F>(base + (size_t)k * XW));
     part = block_sum(part, sh);
     if (threadIdx.x < 32) {  // warp 0 folds the levels, products of a level on separate lanes
-      for (int d = 0; d < 4; d++) acc = lane_double(acc, sm);  // x16 = kChunk
+      for (uint32_t d = 0; d < lv.chunk_log; d++) acc = lane_double(acc, sm);  // x chunk
       acc = lane_add(acc, part, sm);
     }
   }
