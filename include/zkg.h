@@ -74,6 +74,19 @@ int zkg_buf_zeroed(zkg_ctx *ctx, size_t words, zkg_buf **out);
 int zkg_buf_write(zkg_ctx *ctx, zkg_buf *buf, size_t offset_words, const uint32_t *data, size_t words);
 /* Gpu::read / try_read_async (src/gpu.rs:166-199): blocking copy of the first `words` words. */
 int zkg_buf_read(zkg_ctx *ctx, const zkg_buf *buf, uint32_t *out, size_t words);
+
+/* Asynchronous copies (no reference counterpart; wgpu's queue.write_buffer is itself queued).
+ * zkg_buf_write_async queues a host-to-device copy on the context's upload stream: it starts
+ * once the work already queued on the context that uses `buf` has finished (MSM runs, NTTs,
+ * coset shifts, batch launches and asynchronous reads record their buffers), and work queued on
+ * the context after the call waits for it. zkg_buf_read_async queues a device-to-host copy on
+ * the read-back stream that runs after all work queued so far; kernels and writes queued after
+ * it (which may overwrite the buffer) wait for the copy.
+ * Neither call waits: `data` must stay unchanged, and `out` holds the words, only after
+ * zkg_ctx_sync (which waits for both streams). From page-locked host memory (zkg_host_alloc)
+ * the copies overlap the context's kernels. Size errors as zkg_buf_write / zkg_buf_read. */
+int zkg_buf_write_async(zkg_ctx *ctx, zkg_buf *buf, size_t offset_words, const uint32_t *data, size_t words);
+int zkg_buf_read_async(zkg_ctx *ctx, const zkg_buf *buf, uint32_t *out, size_t words);
 /* wgpu Buffer::size / 4 */
 size_t zkg_buf_words(const zkg_buf *buf);
 /* Device address of the buffer, for interop with other CUDA code on the same device. */

@@ -31,6 +31,9 @@ void Batch::check_lane(const void* plan, int lane) {
 
 void Batch::add_msm(MsmPlan* plan, const zkg_buf* bases, const zkg_buf* scalars, zkg_buf* out, int lane) {
   plan->check_buffers(bases, scalars);
+  bufs.push_back(bases);
+  bufs.push_back(scalars);
+  if (out) bufs.push_back(out);
   if (out && out->words < plan->xyzz_words()) fail(ZKG_ESIZE, "result buffer too small for one XYZZ point");
   check_lane(plan, lane);
   Op op;
@@ -45,6 +48,7 @@ void Batch::add_msm(MsmPlan* plan, const zkg_buf* bases, const zkg_buf* scalars,
 
 void Batch::add_ntt(NttPlan* plan, zkg_buf* data, bool inverse, int lane) {
   if (data->words < ((size_t)8 << plan->log_n)) fail(ZKG_ESIZE, "data buffer too small for the transform");
+  bufs.push_back(data);
   check_lane(plan, lane);
   Op op;
   op.kind = inverse ? Op::kNttInverse : Op::kNttForward;
@@ -56,6 +60,7 @@ void Batch::add_ntt(NttPlan* plan, zkg_buf* data, bool inverse, int lane) {
 
 void Batch::add_coset(CosetShift* shift, zkg_buf* data, int lane) {
   if (data->words < ((size_t)8 << shift->log_n)) fail(ZKG_ESIZE, "data buffer too small for the coset shift");
+  bufs.push_back(data);
   if (lane < 0 || lane >= (int)kMaxLanes) fail(ZKG_EINVAL, "lane out of range");
   lanes = std::max(lanes, lane + 1);
   dirty = true;
@@ -148,6 +153,7 @@ void Batch::launch() {
   use(ctx);
   if (dirty || !exec) capture();
   check_cuda(cudaGraphLaunch(exec, ctx->stream), "graph launch");
+  for (const zkg_buf* b : bufs) mark_use(b, ctx->stream);
   // kernels inside the graph are this library's: count them like direct launches
   g_launches.fetch_add(graph_kernels, std::memory_order_relaxed);
 }
@@ -164,6 +170,7 @@ void Batch::run_streams() {
     check_cuda(cudaEventRecord(joins[l], streams[l]), "join");
     check_cuda(cudaStreamWaitEvent(ctx->stream, joins[l], 0), "join wait");
   }
+  for (const zkg_buf* b : bufs) mark_use(b, ctx->stream);
 }
 
 size_t Batch::count_kernels() const {

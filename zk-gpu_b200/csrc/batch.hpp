@@ -27,6 +27,7 @@ struct Batch {
 
   zkg_ctx* ctx;
   std::vector<Op> ops;
+  std::vector<const zkg_buf*> bufs;  // every buffer the operations use (marked at each launch)
   std::map<const void*, int> plan_lane;
   int lanes = 0;
   bool dirty = true;

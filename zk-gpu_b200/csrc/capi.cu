@@ -105,6 +105,11 @@ void zkg_ctx_free(zkg_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
+  for (cudaStream_t s : {ctx->up_stream, ctx->down_stream}) {
+    if (!s) continue;
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
   delete ctx;
 }
 
@@ -113,6 +118,8 @@ int zkg_ctx_sync(zkg_ctx* ctx) {
     need(ctx, "ctx");
     use(ctx);
     check_cuda(cudaStreamSynchronize(ctx->stream), "device work");
+    if (ctx->up_stream) check_cuda(cudaStreamSynchronize(ctx->up_stream), "device work");
+    if (ctx->down_stream) check_cuda(cudaStreamSynchronize(ctx->down_stream), "device work");
     check_cuda(cudaGetLastError(), "device work");
   });
 }
@@ -187,12 +194,65 @@ int zkg_buf_read(zkg_ctx* ctx, const zkg_buf* buf, uint32_t* out, size_t words) 
   });
 }
 
+// One-shot event: `waiter` waits for the work queued on `after` so far.
+static void order_after(cudaStream_t waiter, cudaStream_t after) {
+  cudaEvent_t e;
+  check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventRecord(e, after), "cudaEventRecord");
+  check_cuda(cudaStreamWaitEvent(waiter, e, 0), "cudaStreamWaitEvent");
+  cudaEventDestroy(e);  // released once the wait has been satisfied
+}
+
+// Uploads and read-backs on separate streams (the copy engines of the two directions work in
+// parallel, and a queued read does not hold back the next step's uploads).
+static cudaStream_t side_stream(cudaStream_t* s) {
+  if (!*s) check_cuda(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "cudaStreamCreate");
+  return *s;
+}
+
+int zkg_buf_write_async(zkg_ctx* ctx, zkg_buf* buf, size_t offset_words, const uint32_t* data, size_t words) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(buf, "buf");
+    if (words) need(data, "data");
+    if (offset_words > buf->words || words > buf->words - offset_words)
+      fail(ZKG_ESIZE, "write of " + std::to_string(words) + " words at offset " + std::to_string(offset_words) +
+                          " overruns a buffer of " + std::to_string(buf->words) + " words");
+    use(ctx);
+    if (!words) return;
+    cudaStream_t cs = side_stream(&ctx->up_stream);
+    // after the queued work that still uses the buffer; before any work queued from now on
+    if (buf->last_use) check_cuda(cudaStreamWaitEvent(cs, buf->last_use, 0), "cudaStreamWaitEvent");
+    check_cuda(cudaMemcpyAsync(buf->ptr + offset_words, data, words * 4, cudaMemcpyHostToDevice, cs),
+               "host to device copy");
+    order_after(ctx->stream, cs);
+  });
+}
+
+int zkg_buf_read_async(zkg_ctx* ctx, const zkg_buf* buf, uint32_t* out, size_t words) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(buf, "buf");
+    if (words) need(out, "out");
+    if (words > buf->words)
+      fail(ZKG_ESIZE, "read of " + std::to_string(words) + " words from a buffer of " + std::to_string(buf->words));
+    use(ctx);
+    if (!words) return;
+    cudaStream_t cs = side_stream(&ctx->down_stream);
+    order_after(cs, ctx->stream);  // after the work queued so far (the data's producer)
+    check_cuda(cudaMemcpyAsync(out, buf->ptr, words * 4, cudaMemcpyDeviceToHost, cs), "device to host copy");
+    order_after(ctx->stream, cs);  // kernels queued from now on may overwrite the buffer
+    mark_use(buf, cs);             // and so may later asynchronous writes
+  });
+}
+
 size_t zkg_buf_words(const zkg_buf* buf) { return buf ? buf->words : 0; }
 void* zkg_buf_device_ptr(const zkg_buf* buf) { return buf ? buf->ptr : nullptr; }
 
 void zkg_buf_free(zkg_buf* buf) {
   if (!buf || !buf->owned) return;
   if (buf->ctx) cudaSetDevice(buf->ctx->device);
+  if (buf->last_use) cudaEventDestroy(buf->last_use);
   if (buf->ptr) cudaFree(buf->ptr);
   delete buf;
 }
@@ -276,6 +336,9 @@ int zkg_msm_run(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, cons
     need(bases, "bases");
     need(scalars, "scalars");
     msm->plan.run(bases, scalars);
+    mark_use(bases, msm->plan.ctx->stream);
+    mark_use(scalars, msm->plan.ctx->stream);
+    mark_use(&msm->plan.result_handle, msm->plan.ctx->stream);
     if (result) *result = &msm->plan.result_handle;
   });
 }
@@ -366,6 +429,7 @@ int zkg_ntt_forward(zkg_ntt* ntt, zkg_buf* data) {
     need(ntt, "ntt");
     need(data, "data");
     ntt->plan.run(data, false);
+    mark_use(data, ntt->plan.ctx->stream);
   });
 }
 
@@ -374,6 +438,7 @@ int zkg_ntt_inverse(zkg_ntt* ntt, zkg_buf* data) {
     need(ntt, "ntt");
     need(data, "data");
     ntt->plan.run(data, true);
+    mark_use(data, ntt->plan.ctx->stream);
   });
 }
 
@@ -486,6 +551,7 @@ int zkg_coset_shift(zkg_coset* c, zkg_buf* data) {
     need(c, "coset");
     need(data, "data");
     c->shift.run(data);
+    mark_use(data, c->shift.ctx->stream);
   });
 }
 

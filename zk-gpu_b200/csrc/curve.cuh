@@ -56,7 +56,7 @@ template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_double(const Xyzz<F>& p) {
   F u = dbl(p.y);
   F v, x2, w, s, m2, wy, zz3, zzz3;
-  mul2(u, u, p.x, p.x, v, x2);
+  sqr2(u, p.x, v, x2);
   mul2(u, v, p.x, v, w, s);
   F m = dbl(x2) + x2;
   mul2(m, m, w, p.y, m2, wy);
@@ -87,7 +87,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const Affin
     return xyzz_infinity<F>();
   }
   F ppsq, rr, ppp, q_, zz3, zzz3, t, yppp;
-  mul2(pp, pp, r, r, ppsq, rr);
+  sqr2(pp, r, ppsq, rr);
   mul2(pp, ppsq, p.x, ppsq, ppp, q_);
   F x3 = (rr - ppp) - dbl(q_);
   mul2(r, q_ - x3, p.y, ppp, t, yppp);
@@ -110,7 +110,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) 
     return xyzz_infinity<F>();
   }
   F ppsq, rr, ppp, q_, zz12, zzz12, t, sppp, zz3, zzz3;
-  mul2(pp, pp, r, r, ppsq, rr);
+  sqr2(pp, r, ppsq, rr);
   mul2(pp, ppsq, u1, ppsq, ppp, q_);
   mul2(p.zz, q.zz, p.zzz, q.zzz, zz12, zzz12);
   F x3 = (rr - ppp) - dbl(q_);

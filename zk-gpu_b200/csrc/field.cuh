@@ -544,6 +544,21 @@ __device__ __forceinline__ void mul2(const Fq2T<B>& x, const Fq2T<B>& y, const F
   r2 = Fq2T<B>{ac2 - bd2, (cr2 - ac2) - bd2};
 }
 
+// Two independent squarings. Fq: a pair of products (mul2). Fq2: (a+b)(a-b) and ab per element,
+// two base products instead of three, paired across the two elements.
+template <class P>
+__device__ __forceinline__ void sqr2(const Fp<P>& x, const Fp<P>& y, Fp<P>& rx, Fp<P>& ry) {
+  mul2(x, x, y, y, rx, ry);
+}
+template <class B>
+__device__ __forceinline__ void sqr2(const Fq2T<B>& x, const Fq2T<B>& y, Fq2T<B>& rx, Fq2T<B>& ry) {
+  B re_x, re_y, ab_x, ab_y;
+  mul2(x.a + x.b, x.a - x.b, y.a + y.b, y.a - y.b, re_x, re_y);
+  mul2(x.a, x.b, y.a, y.b, ab_x, ab_y);
+  rx = Fq2T<B>{re_x, ab_x + ab_x};
+  ry = Fq2T<B>{re_y, ab_y + ab_y};
+}
+
 using Fq2 = Fq2T<Fq>;
 using Fq2C = Fq2T<FqC>;
 using Fq2CP = Fq2T<FqCP>;

@@ -66,10 +66,10 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   heads_max = (max_entries + seg_len - 1) / seg_len;
   // Chains of the merge and running-sum levels. Merge: 4 heads per thread (twice the levels of
   // 16, a quarter of the chain; measured faster at every size, G1 2^24 1.43 -> 1.05 ms). Running
-  // sums: chunks of 4 buckets below 2^23 entries, 16 above (more levels cost the window-sum fold
-  // more than the shorter chains save once the first level is large).
+  // sums: chunks of 4 buckets below 2^23 entries, 8 above (measured: reduce + window sums at
+  // G1 2^24 1.30 / 1.20 / 1.25 ms for chunks of 4 / 8 / 16, at 2^16 0.47 / 0.52 / 0.65 ms).
   merge_fan_in = 4;
-  const uint32_t chunk_log = (double)max_entries < (double)(1u << 23) ? 2 : 4;
+  const uint32_t chunk_log = (double)max_entries < (double)(1u << 23) ? 2 : 3;
   size_t len = heads_max;
   merge_levels = 0;
   while (len > 1) {
@@ -92,10 +92,11 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   while (m > 0) {
     if (levels.count >= (uint32_t)kMaxReduceLevels) fail(ZKG_EINVAL, "too many reduction levels");
     uint32_t chunks = (m + chunk - 1) / chunk;
+    uint32_t blocks = (chunks + kReduceThreads - 1) / kReduceThreads;  // one tot point per block
     ms.push_back(m);
-    levels.tot_len[levels.count] = chunks;
+    levels.tot_len[levels.count] = blocks;
     levels.tot_offset[levels.count] = (uint32_t)tot_points;
-    tot_points += (size_t)chunks * windows;
+    tot_points += (size_t)blocks * windows;
     m = chunks - 1;
     levels.count++;
     run_points = std::max<size_t>(run_points, (size_t)m * windows);
@@ -214,9 +215,11 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
         uint32_t m = level_m[l];
         uint32_t chunks = (m + (1u << levels.chunk_log) - 1) >> levels.chunk_log;
         uint32_t* run_out = runs[l & 1].ptr;
-        msm_reduce_level<FC><<<grid_for((size_t)chunks * windows, 128), 128, 0, s>>>(
-            in, in_stride, m, windows, levels.chunk_log, l == 0 ? slot_start.ptr : nullptr,
-            tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(), chunks, run_out, chunks > 1 ? chunks - 1 : 1);
+        const dim3 grid(levels.tot_len[l], windows);
+        msm_reduce_level<FC><<<grid, kReduceThreads, kReduceThreads * sizeof(Xyzz<FC>), s>>>(
+            in, in_stride, m, levels.chunk_log, l == 0 ? slot_start.ptr : nullptr,
+            tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(), levels.tot_len[l], run_out,
+            chunks > 1 ? chunks - 1 : 1);
         check_launch("msm_reduce_level");
         in = run_out;
         in_stride = chunks > 1 ? chunks - 1 : 1;

@@ -53,6 +53,11 @@ struct MsmPlan {
   StageTimer timer;
 
   MsmPlan(zkg_ctx* ctx, int group, size_t n, uint32_t c, uint32_t item_points);
+  ~MsmPlan() {
+    if (result_handle.last_use) cudaEventDestroy(result_handle.last_use);
+  }
+  MsmPlan(const MsmPlan&) = delete;
+  MsmPlan& operator=(const MsmPlan&) = delete;
   size_t xyzz_words() const;
   size_t affine_words() const;
   void check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const;

@@ -13,6 +13,7 @@ constexpr int kScanBlock = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanBlock * kScanItems;
 constexpr int kWindowThreads = 128;
+constexpr int kReduceThreads = 128;  // one running-sum block covers this many chunks of one window
 constexpr int kMaxReduceLevels = 16;
 
 struct ReduceLevels {

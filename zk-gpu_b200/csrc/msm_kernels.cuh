@@ -388,36 +388,6 @@ __global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ sl
 
 // ------------------------------------------------------------------ bucket reduction
 
-// Level of the running-sum reduction. Per window w the input holds m values A_0..A_{m-1} at
-// in + (w * in_stride + b) * XW; level 0 reads the buckets, where an empty slot (no entries)
-// is the point at infinity. With chunk C = 2^chunk_log, thread (w, k) covers b in [Ck, Ck + C):
-//   tot_k = sum_j (j+1) A_{Ck+j}   -> tot_out[w * tot_stride + k]
-//   run_k = sum_j A_{Ck+j}          -> run_out[w * run_stride + k - 1]  (k >= 1)
-template <class F>
-__global__ void __launch_bounds__(128) msm_reduce_level(const uint32_t* __restrict__ in, uint32_t in_stride,
-                                                        uint32_t m, uint32_t windows, uint32_t chunk_log,
-                                                        const uint32_t* __restrict__ slot_start,
-                                                        uint32_t* __restrict__ tot_out, uint32_t tot_stride,
-                                                        uint32_t* __restrict__ run_out, uint32_t run_stride) {
-  constexpr int XW = PointWords<F>::xyzz;
-  const uint32_t chunk = 1u << chunk_log;
-  const uint32_t chunks = (m + chunk - 1) / chunk;
-  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= chunks * windows) return;
-  const uint32_t w = id / chunks, k = id % chunks;
-  const uint32_t lo = k * chunk, hi = min(lo + chunk, m);
-  Xyzz<F> run = xyzz_infinity<F>(), tot = xyzz_infinity<F>();
-  for (uint32_t b = hi; b-- > lo;) {
-    size_t slot = (size_t)w * in_stride + b;
-    bool empty = slot_start && __ldg(&slot_start[slot]) == __ldg(&slot_start[slot + 1]);
-    if (!empty) run = xyzz_add(run, load_xyzz<F>(in + slot * XW));
-    tot = xyzz_add(tot, run);
-  }
-  store_xyzz(tot_out + ((size_t)w * tot_stride + k) * XW, tot);
-  if (k >= 1) store_xyzz(run_out + ((size_t)w * run_stride + k - 1) * XW, run);
-}
-
-
 // Block-wide sum of XYZZ values (one per thread) through shared memory.
 template <class F>
 __device__ Xyzz<F> block_sum(Xyzz<F> v, Xyzz<F>* sh) {
@@ -431,6 +401,43 @@ __device__ Xyzz<F> block_sum(Xyzz<F> v, Xyzz<F>* sh) {
   __syncthreads();
   return r;
 }
+
+
+// Level of the running-sum reduction. Per window w the input holds m values A_0..A_{m-1} at
+// in + (w * in_stride + b) * XW; level 0 reads the buckets, where an empty slot (no entries)
+// is the point at infinity. With chunk C = 2^chunk_log, chunk k of window w (b in [Ck, Ck + C)):
+//   tot_k = sum_j (j+1) A_{Ck+j},  run_k = sum_j A_{Ck+j} -> run_out[w * run_stride + k - 1] (k >= 1).
+// Block (w, j) covers chunks [jT, jT + T) of window w (T = kReduceThreads) and writes the sum of
+// their tot_k to tot_out[w * tot_stride + j]: the window-sum stage then reads one point per
+// block instead of one per chunk.
+template <class F>
+__global__ void __launch_bounds__(kReduceThreads) msm_reduce_level(const uint32_t* __restrict__ in, uint32_t in_stride,
+                                                                   uint32_t m, uint32_t chunk_log,
+                                                                   const uint32_t* __restrict__ slot_start,
+                                                                   uint32_t* __restrict__ tot_out, uint32_t tot_stride,
+                                                                   uint32_t* __restrict__ run_out, uint32_t run_stride) {
+  constexpr int XW = PointWords<F>::xyzz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Xyzz<F>* sh = reinterpret_cast<Xyzz<F>*>(smem_raw);
+  const uint32_t chunk = 1u << chunk_log;
+  const uint32_t chunks = (m + chunk - 1) / chunk;
+  const uint32_t w = blockIdx.y, j = blockIdx.x;
+  const uint32_t k = j * kReduceThreads + threadIdx.x;
+  Xyzz<F> run = xyzz_infinity<F>(), tot = xyzz_infinity<F>();
+  if (k < chunks) {  // no early return: every thread takes part in the block sum below
+    const uint32_t lo = k * chunk, hi = min(lo + chunk, m);
+    for (uint32_t b = hi; b-- > lo;) {
+      size_t slot = (size_t)w * in_stride + b;
+      bool empty = slot_start && __ldg(&slot_start[slot]) == __ldg(&slot_start[slot + 1]);
+      if (!empty) run = xyzz_add(run, load_xyzz<F>(in + slot * XW));
+      tot = xyzz_add(tot, run);
+    }
+    if (k >= 1) store_xyzz(run_out + ((size_t)w * run_stride + k - 1) * XW, run);
+  }
+  tot = block_sum(tot, sh);
+  if (threadIdx.x == 0) store_xyzz(tot_out + ((size_t)w * tot_stride + j) * XW, tot);
+}
+
 
 // One block per window: S_w = sum over levels l of C^l * sum_k tot_l[k] (C = 2^chunk_log),
 // folded from the top level down (chunk_log doublings per level) by warp 0 with lane-parallel

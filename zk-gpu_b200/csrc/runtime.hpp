@@ -53,7 +53,9 @@ inline void check_launch(const char* kernel) {
 
 struct zkg_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // every kernel of the context
+  cudaStream_t up_stream = nullptr;    // asynchronous buffer writes (created on first use)
+  cudaStream_t down_stream = nullptr;  // asynchronous buffer reads (created on first use)
   int sm_count = 0;
   char name[256] = {0};
 };
@@ -63,12 +65,23 @@ struct zkg_buf {
   uint32_t* ptr = nullptr;
   size_t words = 0;
   bool owned = true;  // false for plan-owned results handed out as borrowed handles
+  // Recorded after the last queued work that uses the buffer (a kernel on the context stream
+  // or an asynchronous read): an asynchronous write waits for it (created on first use).
+  cudaEvent_t last_use = nullptr;
 };
 
 namespace zkg {
 
 // Makes the context's device current for this thread.
 inline void use(zkg_ctx* ctx) { check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
+// Notes that work queued on `stream` so far uses `b` (later asynchronous writes wait for it).
+inline void mark_use(const zkg_buf* b, cudaStream_t stream) {
+  if (!b) return;
+  zkg_buf* m = const_cast<zkg_buf*>(b);
+  if (!m->last_use) check_cuda(cudaEventCreateWithFlags(&m->last_use, cudaEventDisableTiming), "cudaEventCreate");
+  check_cuda(cudaEventRecord(m->last_use, stream), "cudaEventRecord");
+}
 
 inline uint32_t* device_alloc(size_t bytes, const char* what) {
   void* p = nullptr;

@@ -55,6 +55,8 @@ SIGNATURES = {
     "zkg_buf_zeroed": (ctypes.c_int, [vp, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "zkg_buf_write": (ctypes.c_int, [vp, vp, ctypes.c_size_t, u32p, ctypes.c_size_t]),
     "zkg_buf_read": (ctypes.c_int, [vp, vp, u32p, ctypes.c_size_t]),
+    "zkg_buf_write_async": (ctypes.c_int, [vp, vp, ctypes.c_size_t, u32p, ctypes.c_size_t]),
+    "zkg_buf_read_async": (ctypes.c_int, [vp, vp, u32p, ctypes.c_size_t]),
     "zkg_buf_words": (ctypes.c_size_t, [vp]),
     "zkg_buf_device_ptr": (vp, [vp]),
     "zkg_buf_free": (None, [vp]),

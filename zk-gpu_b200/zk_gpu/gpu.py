@@ -41,6 +41,14 @@ class Buffer:
         w = as_words(data)
         check(lib().zkg_buf_write(self.gpu.handle, self._h, offset_words, w.ctypes.data_as(u32p), w.size))
 
+    def write_async(self, data: np.ndarray, offset_words: int = 0) -> None:
+        """Queued write (zkg_buf_write_async): `data` (u32 words, ideally page-locked) must stay
+        unchanged until Gpu.wait(); the Gpu keeps a reference until then."""
+        if data.dtype != np.uint32 or not data.flags["C_CONTIGUOUS"]:
+            raise ValueError("write_async needs a contiguous uint32 array")
+        check(lib().zkg_buf_write_async(self.gpu.handle, self._h, offset_words, data.ctypes.data_as(u32p), data.size))
+        self.gpu._pending.append(data)
+
     def free(self) -> None:
         if self._h and self._owned:
             lib().zkg_buf_free(self._h)
@@ -60,6 +68,7 @@ class Gpu:
         h = vp()
         check(lib().zkg_ctx_new(device, ctypes.byref(h)))
         self._h = h.value
+        self._pending = []  # host arrays of queued asynchronous copies, held until wait()
 
     @classmethod
     def new(cls, device: int = 0) -> "Gpu":
@@ -94,9 +103,18 @@ class Gpu:
         check(lib().zkg_buf_read(self._h, buffer.handle, out.ctypes.data_as(u32p), words))
         return out
 
+    def read_async(self, buffer: Buffer, out: np.ndarray) -> None:
+        """Queued read (zkg_buf_read_async) of out.size words into `out` (a contiguous uint32
+        array, ideally page-locked), valid after wait()."""
+        if out.dtype != np.uint32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("read_async needs a contiguous uint32 array")
+        check(lib().zkg_buf_read_async(self._h, buffer.handle, out.ctypes.data_as(u32p), out.size))
+        self._pending.append(out)
+
     def wait(self) -> None:
-        """Gpu::wait: block until all queued work has finished."""
+        """Gpu::wait: block until all queued work (kernels and asynchronous copies) has finished."""
         check(lib().zkg_ctx_sync(self._h))
+        self._pending.clear()
 
     def close(self) -> None:
         if self._h:
