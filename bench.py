@@ -464,9 +464,13 @@ def run_serving(a, gpu) -> dict:
         sv = Server(gpu, lanes=a.serving_lanes, plain=(mode == "plain"))
         for n, g1, g2 in keys:
             sv.add_key(n, g1, g2)
-        # warm every size class once (slot creation, graph capture) outside the timing
+        # warm every size class once (slot creation, graph capture) outside the timing; the
+        # served mode runs several requests of one size at once, so it keeps two slots per size
+        # ready (more are made on its builder thread when a stream needs them)
         for k in sorted(pool):
             sv.wait(sv.submit(pool[k]))
+            if mode == "batched":
+                sv.reserve(k, 2)
         servers[mode] = sv
     for rate in rates:
         rng = np.random.default_rng(int(rate * 1000) + 17)
@@ -475,8 +479,12 @@ def run_serving(a, gpu) -> dict:
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
         point = {"rate_req_per_s": rate, "requests": count}
         for mode in ("plain", "batched"):
+            st0 = servers[mode].stats()
             r = run_stream(servers[mode], [pool[int(k)] for k in ks], arrivals)
+            st1 = servers[mode].stats()
             point[mode] = {key: round(v, 3) for key, v in r.items() if key != "requests"}
+            point[mode]["slots_made"] = st1["slots_created"] - st0["slots_created"]
+            point[mode]["slot_build_ms"] = round(st1["build_ms"] - st0["build_ms"], 1)
         point["throughput_ratio"] = round(point["batched"]["req_per_s"] / point["plain"]["req_per_s"], 3)
         out["points"].append(point)
     for sv in servers.values():

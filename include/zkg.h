@@ -118,9 +118,9 @@ void zkg_msm_free(zkg_msm *msm);
 int zkg_msm_group(const zkg_msm *msm);
 /* Tuning knobs of a plan (no reference counterpart): the accumulation kernel's form, 0 = field
  * products inlined, 1 = products through one out-of-line function (smaller code),
- * 2 = out of line, two independent products per call, 3 / 4 = G1 only: bucket sums in
- * double-precision limbs, products on the FP64 pipe, two per call / one per call (ZKG_EINVAL
- * for G2). Defaults: 4 for G1, 1 for G2.
+ * 2 = out of line, two independent products per call, 3 / 4 = bucket sums in double-precision
+ * limbs, products on the FP64 pipe, two per call / one per call (bit-exact for G1 and G2; the
+ * G2 limb forms spill and are slower). Defaults: 4 for G1, 2 for G2.
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
 /* Counting-sort knob (no reference counterpart): how a warp merges the counting pass's atomics
@@ -229,10 +229,12 @@ size_t zkg_batch_kernels(const zkg_batch *batch);
  *   p <- forward(shift_g(inverse(p))) for p in a, b, c;  h <- (a*b - c) / (g^N - 1);
  *   h <- shift_{1/g}(inverse(h)).
  * Outputs: out_points = 3 G1 XYZZ (32 words each) then 1 G2 XYZZ (64 words); out_h = N elements.
- * Requests queue FIFO and are admitted when a free slot (plans and buffers of their size) exists
- * or a new one fits the HBM budget (idle slots of other sizes are evicted); up to `lanes`
- * requests run at once on separate streams, each as one captured CUDA graph with three parallel
- * branches (continuous batching). plain = 1 is the one-call-at-a-time path: one request at a
+ * Requests queue FIFO; while fewer than `lanes` run, the queue is scanned in order: a request
+ * with an idle slot (plans and buffers of its size) starts at once, one without has a slot made
+ * for it on a builder thread when that fits the HBM budget (idle slots of other sizes are
+ * evicted), and the scan goes on past it; a request whose slot does not fit holds back the ones
+ * behind it. Up to `lanes` requests run at once on separate streams, each as one captured CUDA
+ * graph with three parallel branches (continuous batching). plain = 1 is the one-call-at-a-time path: one request at a
  * time, operations launched one by one. Host buffers of a request must stay valid until
  * zkg_server_wait returns for it, and should be page-locked (zkg_host_alloc) for overlap. */
 typedef struct {
@@ -256,6 +258,7 @@ typedef struct {
 typedef struct {
   uint64_t queued, completed, slots, slots_created, slots_evicted;
   size_t bytes_used, budget;
+  double build_ms; /* host time spent making slots */
 } zkg_server_counters;
 int zkg_server_new(zkg_ctx *ctx, const zkg_server_config *config, zkg_server **out);
 /* Waits for every queued request, then frees the server (keys' buffers stay the caller's). */
@@ -267,6 +270,10 @@ int zkg_server_submit(zkg_server *server, const zkg_proof_request *request, uint
 /* Blocks until the request is done (timeout_ms < 0: no limit; ZKG_ETIMEDOUT otherwise). */
 int zkg_server_wait(zkg_server *server, uint64_t id, int timeout_ms, zkg_request_times *times);
 int zkg_server_stats(zkg_server *server, zkg_server_counters *stats);
+/* Makes idle slots of size 2^log_m until the server holds `count` of them (a warm server: a
+ * burst of requests of that size does not wait for slot construction). ZKG_ENOMEM when a slot
+ * does not fit the HBM budget. */
+int zkg_server_reserve(zkg_server *server, uint32_t log_m, uint32_t count);
 
 /* Largest transform zkg_ntt_noalloc accepts: 2^16 elements. */
 #define ZKG_NTT_NOALLOC_MAX_LOG_N 16

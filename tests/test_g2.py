@@ -86,3 +86,38 @@ def test_g2_full_size_montgomery_upload(gpu, log_n):
     for i in (0, n - 1):
         assert np.array_equal(mont[32 * i: 32 * i + 32],
                               cpu.generator_multiples("G2", k[8 * i: 8 * i + 8], mont256=True))
+
+
+@pytest.mark.parametrize("variant", [1, 3, 4])
+def test_g2_accumulation_forms_agree(gpu, variant):
+    """Integer (one product per call) and double-precision (two / one per call) accumulation on
+    random inputs, repeated bases (doublings) and cancelling pairs."""
+    n = 2000
+    bases = random_points("G2", 70, n).reshape(n, 32)
+    bases[5] = 0
+    bases[10:20] = bases[9]
+    bases = bases.reshape(-1)
+    p = bases[40 * 32: 41 * 32]
+    cases = [random_fr(71, n), fr_words([7] * n), fr_words(i % 5 for i in range(n))]
+    for s in cases:
+        want = msm_ref("G2", bases, s)
+        for c, items in [(10, None), (9, 3)]:
+            assert np.array_equal(gpu_msm(gpu, bases, s, (c, items), G2, variant=variant), want), (variant, c, items)
+    x = 0x1234567890ABCDEF
+    cancel = np.concatenate([p, p, bases[:32 * 6]])
+    cs = np.concatenate([fr_words([x, R - x]), random_fr(72, 6)])
+    assert np.array_equal(gpu_msm(gpu, cancel, cs, (9, None), G2, variant=variant), msm_ref("G2", cancel, cs))
+
+
+@pytest.mark.parametrize("variant", [3, 4])
+def test_g2_full_size_double_precision(gpu, variant):
+    log_n = 20
+    n = 1 << log_n
+    k = uniform_scalars(n, 3100 + log_n)
+    dev = generator_multiples(gpu, G2, k, mont256=True)
+    s = uniform_scalars(n, 4100 + log_n)
+    msm = Msm.for_group(gpu, G2, n, Msm.default_window(n))
+    msm.set_variant(variant)
+    got = affine_words(xyzz_to_affine_g2(gpu.read(msm.run(gpu, dev, gpu.buffer(s)), 64)), G2)
+    gen = np.array(bn254.affine_words("G2", bn254.g2_generator()), dtype=np.uint32)
+    assert np.array_equal(got, cpu.scalar_mul("G2", gen, cpu.fr_dot(s, k)))

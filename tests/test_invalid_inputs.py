@@ -66,9 +66,9 @@ def test_tuning_knobs_reject_out_of_range_values(gpu):
     with pytest.raises(ZkGpuError, match="sort aggregation mode must be 0..3"):
         g1.set_sort(4)
     g2 = Msm.for_group(gpu, Group.G2, 1 << 10, 10)
-    with pytest.raises(ZkGpuError, match="variants 3 and 4 are for G1 only"):
-        g2.set_variant(4)
-    assert g2.params()["variant"] == 1 and g1.params()["variant"] == 4
+    with pytest.raises(ZkGpuError, match="accumulation variant must be 0..4"):
+        g2.set_variant(-1)
+    assert g2.params()["variant"] == 2 and g1.params()["variant"] == 4
     ntt = Ntt(gpu, 12)
     with pytest.raises(ZkGpuError, match="NTT variant must be 0 or 1"):
         ntt.set_variant(2)

@@ -122,3 +122,55 @@ def test_rejects_requests_without_a_key(gpu, key):
     with pytest.raises(ZkGpuError, match="no resident proving key"):
         server.submit(ProofInputs(13))
     server.close()
+
+
+def test_reserved_slots_serve_a_burst_without_new_slots(gpu, key):
+    """reserve() makes idle slots ahead of time; a burst of that many same-size requests runs on
+    them without making more, and the results match the plain path."""
+    reqs = [make_request(11, 7000 + 13 * i) for i in range(3)]
+    alone = run_plain(gpu, key, [make_request(11, 7000 + 13 * i) for i in range(3)])
+    server = Server(gpu, lanes=3, coset_g=G)
+    server.add_key(KEY_N, key[2], key[3])
+    server.reserve(11, 3)
+    server.reserve(11, 2)  # already held: no-op
+    before = server.stats()
+    assert before["slots"] == 3 and before["slots_created"] == 3 and before["build_ms"] > 0
+    ids = [server.submit(r) for r in reqs]
+    for rid in ids:
+        server.wait(rid)
+    after = server.stats()
+    assert after["slots_created"] == 3 and after["completed"] == 3
+    for i, r in enumerate(reqs):
+        assert same_points(affine_points(r.points()), alone[i][0]) and np.array_equal(r.h(), alone[i][1])
+    server.close()
+
+
+def test_requests_with_slots_pass_one_whose_slot_is_being_made(gpu, key):
+    """A request that needs a new slot does not hold back later requests whose slots exist: all
+    complete, with the plain path's results."""
+    sizes = [12, 11, 11, 11]
+    reqs = [make_request(lm, 8000 + 17 * i) for i, lm in enumerate(sizes)]
+    alone = run_plain(gpu, key, [make_request(lm, 8000 + 17 * i) for i, lm in enumerate(sizes)])
+    server = Server(gpu, lanes=4, coset_g=G)
+    server.add_key(KEY_N, key[2], key[3])
+    server.reserve(11, 3)
+    ids = [server.submit(r) for r in reqs]
+    for rid in ids:
+        server.wait(rid)
+    stats = server.stats()
+    assert stats["slots_created"] == 4 and stats["completed"] == 4
+    for i, r in enumerate(reqs):
+        assert same_points(affine_points(r.points()), alone[i][0]) and np.array_equal(r.h(), alone[i][1])
+    server.close()
+
+
+def test_reserve_checks_the_budget_and_the_keys(gpu, key):
+    from zk_gpu import ZkGpuError
+    server = Server(gpu, lanes=2, hbm_budget_bytes=1 << 20, coset_g=G)
+    server.add_key(KEY_N, key[2], key[3])
+    with pytest.raises(ZkGpuError, match="does not fit the HBM budget"):
+        server.reserve(11, 1)
+    with pytest.raises(ZkGpuError, match="no resident proving key"):
+        server.reserve(13, 1)
+    assert server.stats()["bytes_used"] == 0
+    server.close()

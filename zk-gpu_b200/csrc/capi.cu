@@ -308,7 +308,6 @@ int zkg_msm_set_variant(zkg_msm* msm, int variant) {
   return guard([&] {
     need(msm, "msm");
     if (variant < 0 || variant > 4) fail(ZKG_EINVAL, "accumulation variant must be 0..4");
-    if (variant >= 3 && msm->plan.group != ZKG_G1) fail(ZKG_EINVAL, "accumulation variants 3 and 4 are for G1 only");
     msm->plan.acc_variant = variant;
   });
 }
@@ -669,6 +668,13 @@ int zkg_server_stats(zkg_server* s, zkg_server_counters* st) {
     need(s, "server");
     need(st, "stats");
     s->server.stats(st);
+  });
+}
+
+int zkg_server_reserve(zkg_server* s, uint32_t log_m, uint32_t count) {
+  return guard([&] {
+    need(s, "server");
+    s->server.reserve(log_m, count);
   });
 }
 

@@ -12,8 +12,8 @@
 //
 // Reduction: five digit steps in base 2^52, q_i = (t_i mod 2^52) * (-p^-1) mod 2^52; the low half
 // of q_i * p_0 is never formed because t_i + lo(q_i p_0) is the next multiple of 2^52 at or
-// above t_i, so the carry into column i+1 is ceil(t_i / 2^52). Inputs below 2p give an output
-// below 2p (p < 2^254, R = 2^260), so values stay in [0, 2p) between products.
+// above t_i, so the carry into column i+1 is ceil(t_i / 2^52). Inputs whose product is below
+// p 2^260 (any two below 2^256) give an output below 2p (p < 2^254, R = 2^260).
 #pragma once
 #include <cstdint>
 
@@ -253,6 +253,83 @@ __device__ __forceinline__ void mont_mul_tree(const double (&x)[5], const double
   }
 }
 
+// Bias of the reduction phase's patterns in column k (the product phase of mont_mul_sub adds
+// and subtracts equal numbers of patterns, whose biases cancel).
+constexpr int red_lo_terms(int k) {
+  int n = 0;
+  for (int i = 0; i < 5; i++)
+    for (int j = 1; j < 5; j++)
+      if (i + j == k) n++;
+  return n;
+}
+constexpr int red_hi_terms(int k) {
+  int n = 0;
+  for (int i = 0; i < 5; i++)
+    for (int j = 0; j < 5; j++)
+      if (i + j + 1 == k) n++;
+  return n;
+}
+constexpr uint64_t red_bias(int k) { return (uint64_t)red_lo_terms(k) * kB52 + (uint64_t)red_hi_terms(k) * kB104; }
+
+// Column k (base 2^52) of m 2^256, a multiple of m that is at least c d whenever c, d < 2m:
+// m 2^256 = (m << 48) 2^208, so columns 4..9 hold the limbs of m << 48.
+template <class L>
+__host__ __device__ constexpr uint64_t shifted_modulus_limb(int k) {
+  if (k < 4) return 0;
+  const int j = k - 4;
+  const uint64_t lo = j >= 1 ? (L::P(j - 1) >> 4) : 0;            // top 48 bits of limb j-1 -> bits 0..47
+  const uint64_t hi = j < 5 ? ((L::P(j) & 0xfull) << 48) : 0;    // low 4 bits of limb j -> bits 48..51
+  return lo | hi;
+}
+
+// (a b - c d + m 2^256) 2^-260 mod m in one Montgomery reduction: a, b below 4m and c, d below
+// 2m give a result below 1.3m. The columns are signed (the difference of the two products can
+// be negative in any column): carries are ceil(t / 2^52) by arithmetic shifts, and t mod 2^52
+// is the two's complement residue.
+template <typename L>
+__device__ __forceinline__ void mont_mul_sub(const double (&a)[5], const double (&b)[5], const double (&c)[5],
+                                             const double (&d)[5], double (&out)[5]) {
+  int64_t col[10];
+#pragma unroll
+  for (int k = 0; k < 10; k++) col[k] = (int64_t)(shifted_modulus_limb<L>(k) - red_bias(k));
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double h = __fma_rz(a[i], b[j], kC104);
+      const double l = __fma_rn(a[i], b[j], __dsub_rn(kC104p52, h));
+      const double h2 = __fma_rz(c[i], d[j], kC104);
+      const double l2 = __fma_rn(c[i], d[j], __dsub_rn(kC104p52, h2));
+      col[i + j] += (int64_t)(bits(l) - bits(l2));
+      col[i + j + 1] += (int64_t)(bits(h) - bits(h2));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    const int64_t t = col[i];
+    const int64_t carry = (t + (int64_t)kM52) >> 52;  // ceil(t / 2^52), arithmetic shift
+    const double tf = limb_to_double((uint64_t)t & kM52);
+    const double qh = __fma_rz(tf, (double)L::PINV, kC104);
+    const double ql = __fma_rn(tf, (double)L::PINV, __dsub_rn(kC104p52, qh));
+    const double q = __dsub_rn(ql, kC52);
+    col[i + 1] += (int64_t)bits(__fma_rz(q, (double)L::P(0), kC104)) + carry;
+#pragma unroll
+    for (int j = 1; j < 5; j++) {
+      const double h = __fma_rz(q, (double)L::P(j), kC104);
+      const double l = __fma_rn(q, (double)L::P(j), __dsub_rn(kC104p52, h));
+      col[i + j] += (int64_t)bits(l);
+      col[i + j + 1] += (int64_t)bits(h);
+    }
+  }
+  int64_t carry = 0;
+#pragma unroll
+  for (int k = 5; k < 10; k++) {
+    const int64_t v = col[k] + carry;
+    carry = v >> 52;
+    out[k - 5] = limb_to_double(k < 9 ? ((uint64_t)v & kM52) : (uint64_t)v);
+  }
+}
+
 // 8 x 32-bit words (an integer below 2^255) <-> five 52-bit limbs.
 __device__ __forceinline__ void words_to_limbs(const uint32_t (&w)[8], double (&out)[5]) {
   const uint64_t w0 = w[0] | (uint64_t)w[1] << 32, w1 = w[2] | (uint64_t)w[3] << 32;
@@ -410,6 +487,14 @@ __device__ __forceinline__ FqD fqd_mul(const FqD& a, const FqD& b) {
 template <class L = FqLimbs>
 static __device__ __noinline__ FqDPair fqd_mul2_call(FqD a, FqD b, FqD c, FqD d) {
   return FqDPair{fqd_mul<L>(a, b), fqd_mul<L>(c, d)};
+}
+
+// a b - c d (Montgomery form, below 1.3m) for a, b below 4m and c, d below 2m, one call.
+template <class L = FqLimbs>
+static __device__ __noinline__ FqD fqd_mul_sub_call(FqD a, FqD b, FqD c, FqD d) {
+  FqD r;
+  mont_mul_sub<L>(a.l, b.l, c.l, d.l, r.l);
+  return r;
 }
 
 // One product per out-of-line call.

@@ -48,7 +48,7 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   half = 1u << (c - 1);
   slots = (size_t)windows * half;
   seg_len = item_points ? item_points : auto_seg_len(n, windows);
-  acc_variant = group == ZKG_G1 ? 4 : 1;
+  acc_variant = group == ZKG_G1 ? 4 : 2;
   const size_t xw = xyzz_words();
   const size_t max_entries = (size_t)windows * n;
   if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
@@ -159,12 +159,15 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
-      if (acc_variant == 3 && std::is_same<F, Fq>::value)
-        msm_accumulate_f64<true><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
-      else if (acc_variant == 4 && std::is_same<F, Fq>::value)
-        msm_accumulate_f64<false><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      if (acc_variant == 3 || acc_variant == 4) {
+        using E = typename std::conditional<std::is_same<F, Fq>::value, f64::FqD, f64::Fq2D>::type;
+        if (acc_variant == 3)
+          msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, 0, s>>>(
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+        else
+          msm_accumulate_f64<E, false><<<grid_for(heads_max, 128), 128, 0, s>>>(
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      }
       else if (acc_variant == 1)
         msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
             bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);

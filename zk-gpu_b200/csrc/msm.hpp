@@ -32,10 +32,11 @@ struct MsmPlan {
   // Accumulation kernel form: 0 = field products inlined, 1 = through one out-of-line product
   // (smaller code: the inlined mixed addition is thousands of instructions and its warps stall
   // on instruction fetch; measured 17% faster at 2^24), 2 = out of line, independent products
-  // two per call (a further 5% at 2^20 and 2^24 for G1; slower for G2, whose pairs of Fq2
-  // operands no longer fit the argument registers), 3 / 4 = G1 only: bucket arithmetic in
-  // double-precision limbs (msm_f64.cuh), two products per call / one (4: 12% faster than 2
-  // at 2^24). Defaults: 4 for G1, 1 for G2. Tunable.
+  // two per call, 3 / 4 = bucket arithmetic in double-precision limbs (msm_f64.cuh), two
+  // products per call / one. Every form fetches the next base into shared memory with
+  // cp.async. Defaults (measured on B200): 4 for G1 (48.1 ms at 2^24 against 50.1 for 3 and
+  // 59.7 for 2), 2 for G2 (47.4 ms at 2^22 against 48.1 for 1; the limb forms spill for G2).
+  // Tunable.
   int acc_variant = 4;
   // Warp aggregation of the counting pass's atomics (slot_peers in msm_kernels.cuh): 0 = every
   // group of equal slots, 1 = the first lane's group, 2 = none, 3 = the group of the first equal

@@ -295,14 +295,33 @@ __global__ void __launch_bounds__(128) msm_accumulate(const uint32_t* __restrict
   uint32_t head_key = kNoKey;
 
   Xyzz<F> acc = xyzz_infinity<F>();
+  // The next base is fetched into shared memory with cp.async while the current addition runs
+  // (two slots per thread), so the prefetch holds no registers.
+  constexpr int AW = PointWords<F>::affine;  // 16 (G1) or 32 (G2) words
+  __shared__ __align__(16) uint32_t stage[2][128][AW];
+  auto stage_base = [&](uint32_t slot, uint32_t e) {
+    const uint4* g = reinterpret_cast<const uint4*>(bases + (size_t)(e & ~kNegBit) * AW);
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(&stage[slot][threadIdx.x][0]);
+#pragma unroll
+    for (int k = 0; k < AW / 4; k++)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa + 16 * k), "l"(g + k) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
   uint32_t entry = __ldg(&sorted[p0]);
-  Affine<F> next = load_signed_base<F>(bases, entry);
+  uint32_t cur_entry = entry, slot = 0;
+  stage_base(0, entry);
   for (uint32_t p = p0; p < p1; p++) {
-    Affine<F> cur = next;
     if (p + 1 < p1) {
       entry = __ldg(&sorted[p + 1]);
-      next = load_signed_base<F>(bases, entry);
+      stage_base(slot ^ 1, entry);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // this point's copy has landed
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
+    Affine<F> cur = load_affine<F>(&stage[slot][threadIdx.x][0]);
+    if (cur_entry & kNegBit) cur.y = neg(cur.y);
+    cur_entry = entry;
+    slot ^= 1;
     if (p == end) {  // slot s is complete; move to the slot that holds position p
       if (head) {
         store_xyzz(heads + (size_t)t * XW, acc);

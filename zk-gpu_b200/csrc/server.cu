@@ -59,6 +59,7 @@ Server::Server(zkg_ctx* c, const zkg_server_config& config) : ctx(c), cfg(config
     budget = free_b / 10 * 8;
   }
   dispatcher_thread = std::thread([this] { dispatcher(); });
+  builder_thread = std::thread([this] { builder(); });
 }
 
 Server::~Server() {
@@ -68,6 +69,8 @@ Server::~Server() {
   }
   cv.notify_all();
   if (dispatcher_thread.joinable()) dispatcher_thread.join();
+  cv.notify_all();
+  if (builder_thread.joinable()) builder_thread.join();
   cudaSetDevice(ctx->device);
   for (auto& s : slots)
     if (s->stream) cudaStreamSynchronize(s->stream);
@@ -249,72 +252,107 @@ void Server::launch(ServerRequest* r, ServerSlot* s) {
   check_cuda(cudaLaunchHostFunc(st, on_done, r), "completion callback");
 }
 
+// Admission. The queue is scanned in order while lanes are free: a request with an idle slot of
+// its size is launched at once; one without gets a slot built for it by the builder thread when
+// the slot fits the HBM budget (after evicting idle slots of other sizes, oldest first), and
+// the scan goes on, so requests whose slots exist are not held up by a slot under construction.
+// A request whose slot does not fit stops the scan (later requests wait behind it in FIFO order)
+// unless nothing is running, in which case its slot is made anyway.
 void Server::dispatcher() {
   cudaSetDevice(ctx->device);
   for (;;) {
-    ServerRequest* r = nullptr;
-    ServerSlot* slot = nullptr;
-    bool create = false;
-    size_t reserved = 0;
+    std::vector<std::pair<ServerRequest*, ServerSlot*>> ready;
     std::vector<std::unique_ptr<ServerSlot>> victims;
+    bool new_builds = false;
     {
       std::unique_lock<std::mutex> lock(mu);
       for (;;) {
         if (stopping && queue.empty()) return;
-        if (queue.empty()) {
-          cv.wait(lock);
-          continue;
-        }
-        r = queue.front();
-        const uint32_t log_m = r->desc.log_m;
-        int busy = 0;
+        int busy = building;
         for (auto& s : slots) busy += s->busy ? 1 : 0;
-        if (busy >= cfg.lanes) {
-          cv.wait(lock);
-          continue;
-        }
-        for (auto& s : slots)
-          if (!s->busy && s->log_m == log_m) {
-            slot = s.get();
-            break;
-          }
-        if (slot) break;
-        const size_t need = estimate_bytes(log_m);
-        // evict idle slots of other sizes, oldest first, until the new one fits
-        for (size_t i = 0; i < slots.size() && bytes_used + need > budget;) {
-          if (!slots[i]->busy) {
-            bytes_used -= std::min(bytes_used, slots[i]->bytes);
-            victims.push_back(std::move(slots[i]));
-            slots.erase(slots.begin() + i);
-            slots_evicted++;
+        for (auto it = queue.begin(); it != queue.end() && busy < cfg.lanes;) {
+          ServerRequest* r = *it;
+          const uint32_t log_m = r->desc.log_m;
+          ServerSlot* slot = nullptr;
+          for (auto& s : slots)
+            if (!s->busy && s->log_m == log_m) {
+              slot = s.get();
+              break;
+            }
+          if (!slot) {
+            const size_t need = estimate_bytes(log_m);
+            for (size_t i = 0; i < slots.size() && bytes_used + need > budget;) {
+              if (!slots[i]->busy && slots[i]->log_m != log_m) {
+                bytes_used -= std::min(bytes_used, slots[i]->bytes);
+                victims.push_back(std::move(slots[i]));
+                slots.erase(slots.begin() + i);
+                slots_evicted++;
+              } else {
+                i++;
+              }
+            }
+            if (bytes_used + need > budget && busy > 0) break;  // wait for memory, FIFO from here
+            bytes_used += need;
+            builds.emplace_back(r, need);
+            building++;
+            new_builds = true;
           } else {
-            i++;
+            slot->busy = true;
+            slot->req = r;
+            r->slot = slot;
+            ready.emplace_back(r, slot);
           }
+          r->state = 1;
+          r->t_start = now_ms();
+          it = queue.erase(it);
+          busy++;
         }
-        if (bytes_used + need <= budget || busy == 0) {
-          create = true;
-          reserved = need;
-          bytes_used += need;
-          break;
-        }
-        cv.wait(lock);  // wait for a request to finish and free memory
-      }
-      queue.pop_front();
-      r->state = 1;
-      r->t_start = now_ms();
-      if (slot) {
-        slot->busy = true;
-        slot->req = r;
-        r->slot = slot;
+        if (!ready.empty() || new_builds || !victims.empty()) break;
+        cv.wait(lock);
       }
     }
+    if (new_builds) cv.notify_all();
     victims.clear();  // frees device memory outside the lock
-    try {
-      if (create) {
-        std::unique_ptr<ServerSlot> s = make_slot(r->desc.log_m);
+    for (auto& rs : ready) {
+      try {
+        launch(rs.first, rs.second);
+      } catch (const Error& e) {
         std::lock_guard<std::mutex> lock(mu);
-        bytes_used = bytes_used - reserved + s->bytes;
+        rs.second->busy = false;
+        rs.second->req = nullptr;
+        rs.first->state = 3;
+        rs.first->error = e.msg;
+        rs.first->t_done = now_ms();
+        cv.notify_all();
+      }
+    }
+  }
+}
+
+// Makes the slots the dispatcher asked for, one at a time, and launches each waiting request
+// on its new slot.
+void Server::builder() {
+  cudaSetDevice(ctx->device);
+  for (;;) {
+    std::pair<ServerRequest*, size_t> job;
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      cv.wait(lock, [&] { return !builds.empty() || (stopping && queue.empty() && building == 0); });
+      if (builds.empty()) return;
+      job = builds.front();
+      builds.pop_front();
+    }
+    ServerRequest* r = job.first;
+    ServerSlot* slot = nullptr;
+    try {
+      const double t0 = now_ms();
+      std::unique_ptr<ServerSlot> s = make_slot(r->desc.log_m);
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        build_ms += now_ms() - t0;
+        bytes_used = bytes_used - std::min(bytes_used, job.second) + s->bytes;
         slots_created++;
+        building--;
         s->busy = true;
         s->req = r;
         r->slot = s.get();
@@ -324,16 +362,57 @@ void Server::dispatcher() {
       launch(r, slot);
     } catch (const Error& e) {
       std::lock_guard<std::mutex> lock(mu);
-      if (create && !slot) bytes_used -= std::min(bytes_used, reserved);
-      if (slot) {
+      if (!slot) {
+        bytes_used -= std::min(bytes_used, job.second);
+        building--;
+      } else {
         slot->busy = false;
         slot->req = nullptr;
       }
       r->state = 3;
       r->error = e.msg;
       r->t_done = now_ms();
-      cv.notify_all();
     }
+    cv.notify_all();
+  }
+}
+
+// Idle slots of one size made ahead of the requests (so that a burst of requests of that size
+// does not wait for slot construction).
+void Server::reserve(uint32_t log_m, uint32_t count) {
+  if (log_m < 11 || log_m > 26) fail(ZKG_EINVAL, "log_m must be in 11..=26");
+  if (!key_for(log_m)) fail(ZKG_EINVAL, "no resident proving key has 2^" + std::to_string(log_m) + " points");
+  for (;;) {
+    size_t need = 0;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      uint32_t have = 0;
+      for (auto& s : slots) have += s->log_m == log_m ? 1 : 0;
+      if (have >= count) return;
+      need = estimate_bytes(log_m);
+      if (bytes_used + need > budget)
+        fail(ZKG_ENOMEM, "slot of 2^" + std::to_string(log_m) + " does not fit the HBM budget (" +
+                             std::to_string(budget - std::min(budget, bytes_used)) + " bytes left, " +
+                             std::to_string(need) + " needed)");
+      bytes_used += need;
+    }
+    std::unique_ptr<ServerSlot> s;
+    const double t0 = now_ms();
+    try {
+      s = make_slot(log_m);
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(mu);
+      bytes_used -= std::min(bytes_used, need);
+      throw;
+    }
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      build_ms += now_ms() - t0;
+      bytes_used = bytes_used - std::min(bytes_used, need) + s->bytes;
+      slots_created++;
+      slots.push_back(std::move(s));
+    }
+    cv.notify_all();
   }
 }
 
@@ -393,6 +472,7 @@ void Server::stats(zkg_server_counters* s) {
   s->slots_evicted = slots_evicted;
   s->bytes_used = bytes_used;
   s->budget = budget;
+  s->build_ms = build_ms;
 }
 
 }  // namespace zkg

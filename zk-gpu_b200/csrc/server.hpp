@@ -62,13 +62,17 @@ struct Server {
   std::vector<std::unique_ptr<ServerSlot>> slots;
   std::map<uint64_t, std::unique_ptr<ServerRequest>> requests;
   std::deque<ServerRequest*> queue;
+  // admitted requests whose slot is being made, with the bytes reserved for it
+  std::deque<std::pair<ServerRequest*, size_t>> builds;
+  int building = 0;  // slots under construction (each holds a lane)
   size_t bytes_used = 0, budget = 0;
   uint64_t next_id = 1;
   uint64_t slots_created = 0, slots_evicted = 0, completed = 0;
+  double build_ms = 0;
   bool stopping = false;
   std::mutex mu;
-  std::condition_variable cv;  // queue, slot and completion changes
-  std::thread dispatcher_thread;
+  std::condition_variable cv;  // queue, slot, build and completion changes
+  std::thread dispatcher_thread, builder_thread;
 
   Server(zkg_ctx* ctx, const zkg_server_config& cfg);
   ~Server();
@@ -76,10 +80,11 @@ struct Server {
   uint64_t submit(const zkg_proof_request& r);
   int wait(uint64_t id, int timeout_ms, zkg_request_times* times);
   void stats(zkg_server_counters* s);
+  void reserve(uint32_t log_m, uint32_t count);
 
  private:
   void dispatcher();
-  ServerSlot* acquire(std::unique_lock<std::mutex>& lock, uint32_t log_m);
+  void builder();
   std::unique_ptr<ServerSlot> make_slot(uint32_t log_m);
   size_t estimate_bytes(uint32_t log_m) const;
   const ServerKey* key_for(uint32_t log_m) const;

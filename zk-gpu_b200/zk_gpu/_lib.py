@@ -41,7 +41,7 @@ class RequestTimes(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("queued", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("slots", ctypes.c_uint64),
                 ("slots_created", ctypes.c_uint64), ("slots_evicted", ctypes.c_uint64),
-                ("bytes_used", ctypes.c_size_t), ("budget", ctypes.c_size_t)]
+                ("bytes_used", ctypes.c_size_t), ("budget", ctypes.c_size_t), ("build_ms", ctypes.c_double)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/zkg.h
@@ -99,6 +99,7 @@ SIGNATURES = {
     "zkg_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(ProofRequest), ctypes.POINTER(ctypes.c_uint64)]),
     "zkg_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(RequestTimes)]),
     "zkg_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+    "zkg_server_reserve": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_uint32]),
     "zkg_tune_msm": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_size_t, vp, vp, ctypes.c_int,
                                     ctypes.POINTER(MsmTuning), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "zkg_ntt_set_variant": (ctypes.c_int, [vp, ctypes.c_int]),

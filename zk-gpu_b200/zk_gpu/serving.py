@@ -120,6 +120,10 @@ class Server:
         check(lib().zkg_server_wait(self._h, rid, timeout_ms, ctypes.byref(t)))
         return {"queued_ms": t.queued_ms, "device_ms": t.device_ms, "total_ms": t.total_ms}
 
+    def reserve(self, log_m: int, count: int) -> None:
+        """Makes idle slots of size 2^log_m until the server holds `count` of them."""
+        check(lib().zkg_server_reserve(self._h, log_m, count))
+
     def stats(self) -> dict:
         s = ServerStats()
         check(lib().zkg_server_stats(self._h, ctypes.byref(s)))
@@ -138,9 +142,10 @@ class Server:
 
 
 def run_stream(server: Server, requests, arrivals_s) -> dict:
-    """Submits requests[i] at arrivals_s[i] seconds after the start (a request object may be
-    reused only after its previous use completed: pass distinct objects for overlapping
-    requests). Returns requests/s over the whole run and latency percentiles (submit -> done)."""
+    """Submits requests[i] at arrivals_s[i] seconds after the start. Returns requests/s over
+    the whole run and latency percentiles (submit -> done). One request object may appear more
+    than once: its inputs are only read, but overlapping uses write the same output arrays, so
+    its outputs are meaningful only when its uses do not overlap."""
     n = len(requests)
     ids = [None] * n
     lat = [None] * n
