@@ -173,6 +173,10 @@ int zkg_ntt_inverse(zkg_ntt *ntt, zkg_buf *data);
 int zkg_coset_new(zkg_ctx *ctx, uint32_t log_n, const uint32_t *g, zkg_coset **out);
 void zkg_coset_free(zkg_coset *coset);
 int zkg_coset_shift(zkg_coset *coset, zkg_buf *data);
+/* zkg_ntt_inverse then zkg_coset_shift in one call, the shift applied in the inverse's last pass
+ * (its 1/n factor folded into the shift's table): the same words as the two calls, one pass
+ * over the data fewer. The coset must cover 2^log_n elements of the transform. */
+int zkg_ntt_inverse_coset(zkg_ntt *ntt, zkg_buf *data, zkg_coset *coset);
 
 /* ------------------------------------------------------------------ autotuning
  * No reference counterpart (its parameters are fixed: default_window, item size, TILE_LOG).

@@ -170,6 +170,41 @@ def test_coset_evaluation_chain(gpu):
     assert np.array_equal(gpu.read(buf, x.size), x)
 
 
+@pytest.mark.parametrize("log_n", [10, 11, 12, 17, 20])
+def test_inverse_with_fused_coset_shift(gpu, log_n):
+    """inverse_coset (the shift in the inverse's last pass) gives the words of inverse followed
+    by the shift kernel, for one-tile and multi-pass sizes, in both butterfly forms, for two
+    shifts on one plan (their tables are kept apart)."""
+    from zk_gpu import CosetShift
+    x = random_fr(500 + log_n, 1 << log_n)
+    g = np.array(bn254.words32(COSET_G), dtype=np.uint32)
+    ginv = np.array(bn254.words32(pow(COSET_G, R - 2, R)), dtype=np.uint32)
+    want = cpu.coset_shift(cpu.ntt(x, True), g)
+    want_inv = cpu.coset_shift(cpu.ntt(x, True), ginv)
+    ntt = Ntt(gpu, log_n)
+    shift, unshift = CosetShift(gpu, log_n, COSET_G), CosetShift(gpu, log_n, pow(COSET_G, R - 2, R))
+    for variant in (0, 1):
+        ntt.set_variant(variant)
+        for sh, expect in ((shift, want), (unshift, want_inv), (shift, want)):
+            buf = gpu.buffer(x)
+            ntt.inverse_coset(gpu, buf, sh)
+            assert np.array_equal(gpu.read(buf, x.size), expect), f"variant {variant}"
+    # the unfused calls agree word for word
+    buf = gpu.buffer(x)
+    ntt.set_variant(0)
+    ntt.inverse(gpu, buf)
+    shift.shift(gpu, buf)
+    assert np.array_equal(gpu.read(buf, x.size), want)
+
+
+def test_fused_coset_shift_checks_sizes(gpu):
+    from zk_gpu import CosetShift
+    ntt = Ntt(gpu, 12)
+    buf = gpu.empty_buffer(8 << 12)
+    with pytest.raises(ZkGpuError, match="coset shift of 2\\^11 elements on a 2\\^12 transform"):
+        ntt.inverse_coset(gpu, buf, CosetShift(gpu, 11, COSET_G))
+
+
 def test_coset_rejects_bad_generator(gpu):
     from zk_gpu import CosetShift, ZkGpuError
     with pytest.raises(ZkGpuError, match="below r"):

@@ -90,7 +90,11 @@ int zkg_ctx_new(int device, zkg_ctx** out) {
       ctx->sm_count = prop.multiProcessorCount;
       std::strncpy(ctx->name, prop.name, sizeof(ctx->name) - 1);
       check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      int least = 0, greatest = 0;
+      check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+      check_cuda(cudaStreamCreateWithPriority(&ctx->setup, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
     } catch (...) {
+      if (ctx->stream) cudaStreamDestroy(ctx->stream);
       delete ctx;
       throw;
     }
@@ -105,7 +109,7 @@ void zkg_ctx_free(zkg_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
-  for (cudaStream_t s : {ctx->up_stream, ctx->down_stream}) {
+  for (cudaStream_t s : {ctx->up_stream, ctx->down_stream, ctx->setup}) {
     if (!s) continue;
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
@@ -551,6 +555,16 @@ int zkg_coset_shift(zkg_coset* c, zkg_buf* data) {
     need(data, "data");
     c->shift.run(data);
     mark_use(data, c->shift.ctx->stream);
+  });
+}
+
+int zkg_ntt_inverse_coset(zkg_ntt* ntt, zkg_buf* data, zkg_coset* c) {
+  return guard([&] {
+    need(ntt, "ntt");
+    need(data, "data");
+    need(c, "coset");
+    ntt->plan.run(data, true, &c->shift);
+    mark_use(data, ntt->plan.ctx->stream);
   });
 }
 

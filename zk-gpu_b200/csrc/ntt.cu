@@ -11,6 +11,7 @@
 // The first pass reads the caller's buffer into the plan's scratch, middle passes work in
 // place on the scratch, and the last pass writes back in bit-reversed order (fused with the
 // 1/n scaling for the inverse). Transforms of at most 2^11 elements are one tile in one block.
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -52,10 +53,14 @@ __device__ __forceinline__ uint32_t tile_global_index(uint32_t tile, uint32_t sl
 }
 
 // One pass: stages [log_n - lm - s, log_n - lm) on tiles of 2^tl elements.
+// In the last pass of an inverse, sh_hi / sh_lo (when not null) apply a coset shift: output
+// element i (natural order) is multiplied by sh_hi[i >> sh_bits] * sh_lo[i mod 2^sh_bits], the
+// low table already holding n^-1 g^j, so the shift replaces the 1/n scaling.
 template <bool LAST>
 __global__ void __launch_bounds__(kNttThreads, 3)
     ntt_pass(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const uint32_t* __restrict__ tw,
-             uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale) {
+             uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale,
+             const uint32_t* __restrict__ sh_hi, const uint32_t* __restrict__ sh_lo, uint32_t sh_bits) {
   extern __shared__ __align__(16) uint32_t tile_words[];
   const uint32_t lg = tl - s;
   const uint32_t tile = blockIdx.x;
@@ -94,9 +99,15 @@ __global__ void __launch_bounds__(kNttThreads, 3)
 
   for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
     Fr v = load_fe<Fr>(tile_words + 8 * slot);
-    if (scale_flag) v = v * scale;
     uint32_t g = tile_global_index(tile, slot, lg, lm, s);
     if (LAST) g = __brev(g) >> (32 - log_n);
+    if (LAST && sh_hi != nullptr) {
+      const Fr gi = load_fe<Fr>(sh_hi + 8 * (size_t)(g >> sh_bits)) *
+                    load_fe<Fr>(sh_lo + 8 * (size_t)(g & ((1u << sh_bits) - 1)));
+      v = v * gi;
+    } else if (scale_flag) {
+      v = v * scale;
+    }
     store_fe(dst + 8 * (size_t)g, v);
   }
 }
@@ -248,8 +259,10 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   host::words32(n_inv, n_inv_words);
 
   scratch.alloc(8 * n, "ntt scratch");
-  build_twiddles(w, fwd_tw);
-  build_twiddles(w_inv, inv_tw);
+  build_twiddles(w, fwd_tw, seeds[0]);
+  build_twiddles(w_inv, inv_tw, seeds[1]);
+  // Set-up work runs on the set-up stream: done before the plan is used on any stream.
+  check_cuda(cudaStreamSynchronize(ctx->setup), "ntt twiddles");
   const size_t smem = (size_t)32 << (log_n < kTileLog ? log_n : kTileLog);
   check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
@@ -267,13 +280,13 @@ bool NttPlan::set_variant(int v) {
     use(ctx);
     fwd_twd.alloc(10 * count, "ntt twiddle limbs");
     inv_twd.alloc(10 * count, "ntt twiddle limbs");
-    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->stream>>>(fwd_tw.ptr, count,
+    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->setup>>>(fwd_tw.ptr, count,
                                                                         reinterpret_cast<double*>(fwd_twd.ptr));
     check_launch("ntt_twiddles_to_limbs");
-    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->stream>>>(inv_tw.ptr, count,
+    ntt_twiddles_to_limbs<<<grid_for(count, 256), 256, 0, ctx->setup>>>(inv_tw.ptr, count,
                                                                         reinterpret_cast<double*>(inv_twd.ptr));
     check_launch("ntt_twiddles_to_limbs");
-    check_cuda(cudaStreamSynchronize(ctx->stream), "ntt twiddle limbs");  // enqueue may use another stream
+    check_cuda(cudaStreamSynchronize(ctx->setup), "ntt twiddle limbs");
   }
   variant = v;
   // Pass split: one tile when it fits, else passes of near-equal size, at most 9 stages each
@@ -298,7 +311,7 @@ bool NttPlan::set_max_stages(uint32_t ms) {
   return true;
 }
 
-void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out) {
+void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]) {
   const host::Field& f = host::fr();
   const size_t count = (size_t)1 << (log_n - 1);
   const uint32_t lo_bits = (log_n - 1 + 1) / 2;  // ceil((log_n - 1) / 2)
@@ -307,19 +320,61 @@ void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out) {
   std::vector<uint32_t> lo = powers_words(root, lo_len);
   host::U256 step = host::pow(root, host::U256{{(uint64_t)lo_len, 0, 0, 0}}, f);
   std::vector<uint32_t> hi = powers_words(step, hi_len);
-  DeviceArray dlo, dhi;
+  DeviceArray& dlo = seed[0];
+  DeviceArray& dhi = seed[1];
   dlo.alloc(lo.size(), "ntt twiddle seeds");
   dhi.alloc(hi.size(), "ntt twiddle seeds");
-  check_cuda(cudaMemcpyAsync(dlo.ptr, lo.data(), lo.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "twiddle copy");
-  check_cuda(cudaMemcpyAsync(dhi.ptr, hi.data(), hi.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "twiddle copy");
+  // From pageable host memory: the call returns once the host vectors have been staged.
+  check_cuda(cudaMemcpyAsync(dlo.ptr, lo.data(), lo.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "twiddle copy");
+  check_cuda(cudaMemcpyAsync(dhi.ptr, hi.data(), hi.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "twiddle copy");
   out.alloc(8 * count, "ntt twiddles");
-  ntt_twiddles<<<grid_for(count, 256), 256, 0, ctx->stream>>>(dhi.ptr, dlo.ptr, lo_bits, count, out.ptr);
+  ntt_twiddles<<<grid_for(count, 256), 256, 0, ctx->setup>>>(dhi.ptr, dlo.ptr, lo_bits, count, out.ptr);
   check_launch("ntt_twiddles");
-  // The seed arrays are freed when this function returns: wait for the kernel first.
-  check_cuda(cudaStreamSynchronize(ctx->stream), "ntt twiddles");
 }
 
-void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
+// lo'[j] = lo[j] * f (Montgomery products), j < len.
+__global__ void scale_powers_kernel(const uint32_t* __restrict__ lo, size_t len, Fr f, uint32_t* __restrict__ out) {
+  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= len) return;
+  store_fe(out + 8 * j, load_fe<Fr>(lo + 8 * j) * f);
+}
+
+const NttPlan::FusedShift* NttPlan::fused_for(const CosetShift& shift) {
+  for (auto& f : fused)
+    if (f->serial == shift.serial) return f.get();
+  if (shift.log_n != log_n)
+    fail(ZKG_EINVAL, "coset shift of 2^" + std::to_string(shift.log_n) + " elements on a 2^" + std::to_string(log_n) +
+                         " transform");
+  std::unique_ptr<FusedShift> f(new FusedShift);
+  f->serial = shift.serial;
+  const size_t len = (size_t)1 << shift.lo_bits;
+  f->lo.alloc(8 * len, "fused coset table");
+  Fr inv_n;
+  std::memcpy(inv_n.w, n_inv_words, sizeof(inv_n.w));
+  use(ctx);
+  scale_powers_kernel<<<grid_for(len, 256), 256, 0, ctx->setup>>>(shift.lo.ptr, len, inv_n, f->lo.ptr);
+  check_launch("scale_powers_kernel");
+  // Set-up work runs on the set-up stream: done before the plan uses the table on any stream.
+  check_cuda(cudaStreamSynchronize(ctx->setup), "fused coset table");
+  fused.push_back(std::move(f));
+  return fused.back().get();
+}
+
+void NttPlan::prepare_shift(const CosetShift& shift) {
+  if (variant == 0) fused_for(shift);
+}
+
+void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift) {
+  if (shift && !inverse) fail(ZKG_EINVAL, "a fused coset shift follows an inverse transform");
+  if (shift && variant == 1) {  // double-precision form: the shift as its own kernel
+    enqueue(data, inverse, s);
+    const_cast<CosetShift*>(shift)->enqueue(data, s);
+    return;
+  }
+  const FusedShift* fs = shift ? fused_for(*shift) : nullptr;
+  const uint32_t* sh_hi = fs ? shift->hi.ptr : nullptr;
+  const uint32_t* sh_lo = fs ? fs->lo.ptr : nullptr;
+  const uint32_t sh_bits = fs ? shift->lo_bits : 0;
   const uint32_t* tw = inverse ? inv_tw.ptr : fwd_tw.ptr;
   const double* twd = reinterpret_cast<const double*>(inverse ? inv_twd.ptr : fwd_twd.ptr);
   Fr scale;
@@ -343,9 +398,11 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
     else if (variant == 1)
       ntt_pass_f64<false><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale);
     else if (last)
-      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale, sh_hi,
+                                                      sh_lo, sh_bits);
     else
-      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale, nullptr,
+                                                       nullptr, 0);
     check_launch("ntt_pass");
     if (timer.enabled) timer.end(ev, s);
     done += st;
@@ -353,14 +410,14 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s) {
   if (timer.enabled) timer.runs++;
 }
 
-void NttPlan::run(zkg_buf* data, bool inverse) {
+void NttPlan::run(zkg_buf* data, bool inverse, const CosetShift* shift) {
   const size_t need = (size_t)32 << log_n;
   const size_t have = data->words * 4;
   if (have < need)
     fail(ZKG_ESIZE, "data buffer holds " + std::to_string(have) + " bytes; a 2^" + std::to_string(log_n) +
                         " transform needs " + std::to_string(need));
   use(ctx);
-  enqueue(data->ptr, inverse, ctx->stream);
+  enqueue(data->ptr, inverse, ctx->stream, shift);
 }
 
 }  // namespace zkg
@@ -381,7 +438,10 @@ __global__ void coset_shift_kernel(uint32_t* __restrict__ data, size_t n, const 
   store_fe(data + 8 * i, load_fe<Fr>(data + 8 * i) * p);
 }
 
-CosetShift::CosetShift(zkg_ctx* c, uint32_t log_n_, const uint32_t* g_plain) : ctx(c), log_n(log_n_) {
+static std::atomic<uint64_t> g_coset_serial{1};
+
+CosetShift::CosetShift(zkg_ctx* c, uint32_t log_n_, const uint32_t* g_plain)
+    : ctx(c), log_n(log_n_), serial(g_coset_serial.fetch_add(1)) {
   if (log_n < 1 || log_n > 28) fail(ZKG_EINVAL, "log_n must be in 1..=28");
   use(ctx);
   const host::Field& f = host::fr();
@@ -396,9 +456,10 @@ CosetShift::CosetShift(zkg_ctx* c, uint32_t log_n_, const uint32_t* g_plain) : c
   std::vector<uint32_t> hi_h = powers_words(host::pow(g, host::U256{{(uint64_t)lo_len, 0, 0, 0}}, f), hi_len);
   lo.alloc(lo_h.size(), "coset powers");
   hi.alloc(hi_h.size(), "coset powers");
-  check_cuda(cudaMemcpyAsync(lo.ptr, lo_h.data(), lo_h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
-  check_cuda(cudaMemcpyAsync(hi.ptr, hi_h.data(), hi_h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
-  check_cuda(cudaStreamSynchronize(ctx->stream), "coset powers");  // host vectors die on return
+  check_cuda(cudaMemcpyAsync(lo.ptr, lo_h.data(), lo_h.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "copy");
+  check_cuda(cudaMemcpyAsync(hi.ptr, hi_h.data(), hi_h.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "copy");
+  // Set-up work runs on the set-up stream: done before the shift is used on any stream.
+  check_cuda(cudaStreamSynchronize(ctx->setup), "coset powers");
 }
 
 void CosetShift::enqueue(uint32_t* data, cudaStream_t s) {
@@ -539,9 +600,11 @@ static void ntt_noalloc(uint32_t log_n, int inverse, uint32_t* data, cudaStream_
     uint32_t* dst = last ? data : pingpong;
     const int scale_flag = last && inverse;
     if (last)
-      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale, nullptr,
+                                                      nullptr, 0);
     else
-      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass<false><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale, nullptr,
+                                                       nullptr, 0);
     check_launch("ntt_pass");
     done += st;
   }

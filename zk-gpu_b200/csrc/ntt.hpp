@@ -1,11 +1,14 @@
 // NTT plan (host side of Ntt, src/ntt.rs:14-119).
 #pragma once
+#include <memory>
 #include <vector>
 
 #include "host_field.hpp"
 #include "runtime.hpp"
 
 namespace zkg {
+
+struct CosetShift;
 
 struct NttPlan {
   zkg_ctx* ctx;
@@ -14,12 +17,16 @@ struct NttPlan {
   uint32_t n_inv_words[8];       // 1/n in Montgomery form
   // twiddles w^j, j < n/2: 8 words (R = 2^256) and five double limbs (R = 2^260) each
   DeviceArray scratch, fwd_tw, inv_tw, fwd_twd, inv_twd;
+  // Seeds of the twiddle tables (two short tables of powers per direction), kept for the
+  // plan's lifetime: freeing them would synchronise the whole device, which stalls a plan
+  // made while other work runs (a server slot made under load).
+  DeviceArray seeds[2][2];
   StageTimer timer;  // one stage id per pass
 
   NttPlan(zkg_ctx* ctx, uint32_t log_n);
   // Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs (measured
   // 12% slower at 2^24 on B200; the tuner may still pick it). Resets the pass split to the
-  // form's default. The first switch to form 1 builds its twiddle limbs on the plan's stream.
+  // form's default. The first switch to form 1 builds its twiddle limbs (set-up stream, waited for).
   bool set_variant(int variant);
   int variant = 0;
   uint32_t tile_log() const;
@@ -27,18 +34,32 @@ struct NttPlan {
   // (transforms of one tile have a single pass).
   bool set_max_stages(uint32_t max_stages);
   uint32_t max_stages = 9;
-  // Queues one transform of data (2^log_n elements) on stream s.
-  void enqueue(uint32_t* data, bool inverse, cudaStream_t s);
-  void run(zkg_buf* data, bool inverse);
+  // Queues one transform of data (2^log_n elements) on stream s. With `shift` (inverse only),
+  // the coset shift x_i <- x_i * g^i of that object is applied in the transform's last pass
+  // (the same result as the transform followed by shift->enqueue, without another pass over
+  // the data); the double-precision form runs the shift as its own kernel.
+  void enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift = nullptr);
+  void run(zkg_buf* data, bool inverse, const CosetShift* shift = nullptr);
+  // Builds (on the set-up stream, then waits) the table a fused shift needs: the shift's
+  // low powers times 1/n. enqueue makes it on first use; call this first when enqueue will be
+  // captured into a graph.
+  void prepare_shift(const CosetShift& shift);
 
  private:
-  void build_twiddles(const host::U256& root, DeviceArray& out);
+  void build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]);
+  struct FusedShift {
+    uint64_t serial;
+    DeviceArray lo;  // n^-1 g^j, Montgomery form
+  };
+  std::vector<std::unique_ptr<FusedShift>> fused;
+  const FusedShift* fused_for(const CosetShift& shift);
 };
 
 // x_i <- x_i * g^i over the first 2^log_n elements (plain Fr words), g fixed per object.
 struct CosetShift {
   zkg_ctx* ctx;
   uint32_t log_n, lo_bits = 0;
+  uint64_t serial;  // unique per object (keys the transforms' fused tables)
   DeviceArray hi, lo;  // powers g^(k * 2^lo_bits) and g^j, Montgomery form
   CosetShift(zkg_ctx* ctx, uint32_t log_n, const uint32_t* g_plain);
   void enqueue(uint32_t* data, cudaStream_t s);

@@ -56,6 +56,11 @@ struct zkg_ctx {
   cudaStream_t stream = nullptr;       // every kernel of the context
   cudaStream_t up_stream = nullptr;    // asynchronous buffer writes (created on first use)
   cudaStream_t down_stream = nullptr;  // asynchronous buffer reads (created on first use)
+  // One-time set-up work of plans (twiddle and power tables), waited for by the constructor.
+  // Highest stream priority: the hardware hands its blocks out before those of kernels already
+  // queued, so a plan made while the device is busy (a server slot made under load) does not
+  // wait for all of that work.
+  cudaStream_t setup = nullptr;
   int sm_count = 0;
   char name[256] = {0};
 };

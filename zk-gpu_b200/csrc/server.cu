@@ -138,6 +138,8 @@ std::unique_ptr<ServerSlot> Server::make_slot(uint32_t log_m) {
     host::words32(gi, w);
     s->unshift.reset(new CosetShift(ctx, log_m + 1, w));
   }
+  s->ntt->prepare_shift(*s->shift);  // tables of the fused shifts, made before graph capture
+  s->ntt->prepare_shift(*s->unshift);
   for (auto& b : s->sg1) b.alloc(8 * m, "server scalars");
   s->sg2.alloc(8 * m, "server scalars");
   for (auto& p : s->poly) p.alloc(8 * N, "server polynomials");
@@ -196,13 +198,11 @@ void Server::enqueue_work(ServerSlot* s, cudaStream_t main, cudaStream_t b0, cud
   // witness-map chain
   const uint32_t log_n = s->log_m + 1;
   for (int j = 0; j < 3; j++) {
-    s->ntt->enqueue(s->poly[j].ptr, true, b1);
-    s->shift->enqueue(s->poly[j].ptr, b1);
+    s->ntt->enqueue(s->poly[j].ptr, true, b1, s->shift.get());  // inverse, then shift by g in its last pass
     s->ntt->enqueue(s->poly[j].ptr, false, b1);
   }
   quotient(s->poly[0].ptr, s->poly[1].ptr, s->poly[2].ptr, log_n, coset_zinv(cfg.coset_g, log_n), b1);
-  s->ntt->enqueue(s->poly[0].ptr, true, b1);
-  s->unshift->enqueue(s->poly[0].ptr, b1);
+  s->ntt->enqueue(s->poly[0].ptr, true, b1, s->unshift.get());
   if (fork) {
     check_cuda(cudaEventRecord(s->join[0], b0), "join");
     check_cuda(cudaEventRecord(s->join[1], b1), "join");

@@ -84,6 +84,7 @@ SIGNATURES = {
     "zkg_coset_new": (ctypes.c_int, [vp, ctypes.c_uint32, u32p, ctypes.POINTER(vp)]),
     "zkg_coset_free": (None, [vp]),
     "zkg_coset_shift": (ctypes.c_int, [vp, vp]),
+    "zkg_ntt_inverse_coset": (ctypes.c_int, [vp, vp, vp]),
     "zkg_batch_new": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
     "zkg_batch_free": (None, [vp]),
     "zkg_batch_add_msm": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int]),

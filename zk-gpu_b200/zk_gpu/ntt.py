@@ -37,6 +37,10 @@ class Ntt:
         """In-place inverse transform, including the 1/n factor."""
         check(lib().zkg_ntt_inverse(self._h, data.handle))
 
+    def inverse_coset(self, gpu: Gpu, data: Buffer, coset: "CosetShift") -> None:
+        """inverse() then coset.shift() in one call: the shift runs in the inverse's last pass."""
+        check(lib().zkg_ntt_inverse_coset(self._h, data.handle, coset.handle))
+
     def set_variant(self, variant: int) -> None:
         """Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs."""
         check(lib().zkg_ntt_set_variant(self._h, variant))
