@@ -80,8 +80,10 @@ int zkg_buf_read(zkg_ctx *ctx, const zkg_buf *buf, uint32_t *out, size_t words);
  * once the work already queued on the context that uses `buf` has finished (MSM runs, NTTs,
  * coset shifts, batch launches and asynchronous reads record their buffers), and work queued on
  * the context after the call waits for it. zkg_buf_read_async queues a device-to-host copy on
- * the read-back stream that runs after all work queued so far; kernels and writes queued after
- * it (which may overwrite the buffer) wait for the copy.
+ * the read-back stream that runs after the last queued work that uses `buf` (every entry point
+ * that queues work on a buffer records it); work queued after it that writes `buf` (an NTT or
+ * coset shift of it, an MSM run of the plan whose result it is, a batch that holds it, a
+ * write) waits for the copy, other work runs alongside it.
  * Neither call waits: `data` must stay unchanged, and `out` holds the words, only after
  * zkg_ctx_sync (which waits for both streams). From page-locked host memory (zkg_host_alloc)
  * the copies overlap the context's kernels. Size errors as zkg_buf_write / zkg_buf_read. */

@@ -116,3 +116,51 @@ def test_next_upload_waits_for_a_queued_read_of_the_buffer(gpu):
     gpu.wait()
     assert np.array_equal(out.array, cpu.ntt(x))
     assert np.array_equal(back.array, y)
+
+
+def test_read_back_overlaps_later_work_but_not_later_writers(gpu):
+    """A read of an NTT output does not hold back an MSM queued after it, but the next transform
+    of the same buffer (which overwrites it) waits for the read; the MSM plan's result is read
+    before the next run of that plan overwrites it."""
+    log_n, n = 16, 1 << 14
+    x, y = random_fr(20, 1 << log_n), random_fr(21, 1 << log_n)
+    bases = random_points("G1", 22, n)
+    s1, s2 = random_fr(23, n), random_fr(24, n)
+    base_buf, sbuf1, sbuf2 = Msm.upload_bases(gpu, bases), gpu.buffer(s1), gpu.buffer(s2)
+    ntt = Ntt(gpu, log_n)
+    msm = Msm(gpu, n, Msm.default_window(n))
+    data = gpu.buffer(x)
+    fwd_x, fwd_y = PinnedWords(x.size), PinnedWords(x.size)
+    res1, res2 = PinnedWords(32), PinnedWords(32)
+    new = pinned(y)
+    for _ in range(2):
+        ntt.forward(gpu, data)
+        gpu.read_async(data, fwd_x.array)    # read of the first transform's output
+        r = msm.run(gpu, base_buf, sbuf1)    # independent work: runs alongside the read
+        gpu.read_async(r, res1.array)
+        r = msm.run(gpu, base_buf, sbuf2)    # overwrites the plan's result: waits for that read
+        gpu.read_async(r, res2.array)
+        data.write_async(new.array)          # overwrites data: waits for the first read
+        ntt.forward(gpu, data)
+        gpu.read_async(data, fwd_y.array)
+        ntt.inverse(gpu, data)               # overwrites data: waits for the second read
+        gpu.wait()
+        assert np.array_equal(fwd_x.array, cpu.ntt(x))
+        assert np.array_equal(fwd_y.array, cpu.ntt(y))
+        assert np.array_equal(gpu.read(data, y.size), y)
+        assert np.array_equal(affine_words(xyzz_to_affine(res1.array)), msm_ref("G1", bases, s1))
+        assert np.array_equal(affine_words(xyzz_to_affine(res2.array)), msm_ref("G1", bases, s2))
+        data.write(x)
+
+
+def test_synchronous_write_then_queued_read(gpu):
+    """A blocking write from pageable memory followed by a queued read returns the new words."""
+    buf = gpu.buffer(random_fr(25, 4096))
+    y = random_fr(26, 4096)
+    out = PinnedWords(y.size)
+    ntt = Ntt(gpu, 12)
+    ntt.forward(gpu, buf)          # an older recorded use of the buffer
+    buf.write(y)
+    gpu.read_async(buf, out.array)
+    gpu.wait()
+    assert np.array_equal(out.array, y)

@@ -33,6 +33,7 @@ void Batch::add_msm(MsmPlan* plan, const zkg_buf* bases, const zkg_buf* scalars,
   plan->check_buffers(bases, scalars);
   bufs.push_back(bases);
   bufs.push_back(scalars);
+  bufs.push_back(&plan->result_handle);  // the plan's own result, written by the batch too
   if (out) bufs.push_back(out);
   if (out && out->words < plan->xyzz_words()) fail(ZKG_ESIZE, "result buffer too small for one XYZZ point");
   check_lane(plan, lane);
@@ -152,6 +153,7 @@ void Batch::capture() {
 void Batch::launch() {
   use(ctx);
   if (dirty || !exec) capture();
+  for (const zkg_buf* b : bufs) wait_reads(b, ctx->stream);
   check_cuda(cudaGraphLaunch(exec, ctx->stream), "graph launch");
   for (const zkg_buf* b : bufs) mark_use(b, ctx->stream);
   // kernels inside the graph are this library's: count them like direct launches
@@ -163,6 +165,7 @@ void Batch::launch() {
 void Batch::run_streams() {
   use(ctx);
   ensure_streams();
+  for (const zkg_buf* b : bufs) wait_reads(b, ctx->stream);
   check_cuda(cudaEventRecord(fork, ctx->stream), "fork");
   for (int l = 0; l < lanes; l++) {
     check_cuda(cudaStreamWaitEvent(streams[l], fork, 0), "fork wait");

@@ -180,7 +180,9 @@ int zkg_buf_write(zkg_ctx* ctx, zkg_buf* buf, size_t offset_words, const uint32_
       fail(ZKG_ESIZE, "write of " + std::to_string(words) + " words at offset " + std::to_string(offset_words) +
                           " overruns a buffer of " + std::to_string(buf->words) + " words");
     use(ctx);
+    wait_reads(buf, ctx->stream);
     copy_in(ctx, buf->ptr + offset_words, data, words);
+    if (words) mark_use(buf, ctx->stream);
   });
 }
 
@@ -230,6 +232,7 @@ int zkg_buf_write_async(zkg_ctx* ctx, zkg_buf* buf, size_t offset_words, const u
     check_cuda(cudaMemcpyAsync(buf->ptr + offset_words, data, words * 4, cudaMemcpyHostToDevice, cs),
                "host to device copy");
     order_after(ctx->stream, cs);
+    mark_use(buf, cs);  // an asynchronous read queued next reads the new data
   });
 }
 
@@ -243,10 +246,19 @@ int zkg_buf_read_async(zkg_ctx* ctx, const zkg_buf* buf, uint32_t* out, size_t w
     use(ctx);
     if (!words) return;
     cudaStream_t cs = side_stream(&ctx->down_stream);
-    order_after(cs, ctx->stream);  // after the work queued so far (the data's producer)
+    // after the data's producer: the buffer's last recorded use (every entry point that queues
+    // work on a buffer records one), else all the work queued so far
+    if (buf->last_use)
+      check_cuda(cudaStreamWaitEvent(cs, buf->last_use, 0), "cudaStreamWaitEvent");
+    else
+      order_after(cs, ctx->stream);
     check_cuda(cudaMemcpyAsync(out, buf->ptr, words * 4, cudaMemcpyDeviceToHost, cs), "device to host copy");
-    order_after(ctx->stream, cs);  // kernels queued from now on may overwrite the buffer
-    mark_use(buf, cs);             // and so may later asynchronous writes
+    // work that writes the buffer later waits for this read; other work runs alongside it
+    zkg_buf* m = const_cast<zkg_buf*>(buf);
+    if (!m->pending_read)
+      check_cuda(cudaEventCreateWithFlags(&m->pending_read, cudaEventDisableTiming), "cudaEventCreate");
+    check_cuda(cudaEventRecord(m->pending_read, cs), "cudaEventRecord");
+    mark_use(buf, cs);  // and so do later asynchronous writes
   });
 }
 
@@ -257,6 +269,7 @@ void zkg_buf_free(zkg_buf* buf) {
   if (!buf || !buf->owned) return;
   if (buf->ctx) cudaSetDevice(buf->ctx->device);
   if (buf->last_use) cudaEventDestroy(buf->last_use);
+  if (buf->pending_read) cudaEventDestroy(buf->pending_read);
   if (buf->ptr) cudaFree(buf->ptr);
   delete buf;
 }
@@ -338,6 +351,7 @@ int zkg_msm_run(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, cons
     need(msm, "msm");
     need(bases, "bases");
     need(scalars, "scalars");
+    wait_reads(&msm->plan.result_handle, msm->plan.ctx->stream);
     msm->plan.run(bases, scalars);
     mark_use(bases, msm->plan.ctx->stream);
     mark_use(scalars, msm->plan.ctx->stream);
@@ -352,7 +366,9 @@ int zkg_msm_profile(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, 
     need(msm, "msm");
     need(bases, "bases");
     need(scalars, "scalars");
+    wait_reads(&msm->plan.result_handle, msm->plan.ctx->stream);
     auto times = msm->plan.profile(bases, scalars);
+    mark_use(&msm->plan.result_handle, msm->plan.ctx->stream);
     size_t k = 0;
     for (auto& t : times) {
       if (k >= cap || !out) break;
@@ -431,6 +447,7 @@ int zkg_ntt_forward(zkg_ntt* ntt, zkg_buf* data) {
   return guard([&] {
     need(ntt, "ntt");
     need(data, "data");
+    wait_reads(data, ntt->plan.ctx->stream);
     ntt->plan.run(data, false);
     mark_use(data, ntt->plan.ctx->stream);
   });
@@ -440,6 +457,7 @@ int zkg_ntt_inverse(zkg_ntt* ntt, zkg_buf* data) {
   return guard([&] {
     need(ntt, "ntt");
     need(data, "data");
+    wait_reads(data, ntt->plan.ctx->stream);
     ntt->plan.run(data, true);
     mark_use(data, ntt->plan.ctx->stream);
   });
@@ -553,6 +571,7 @@ int zkg_coset_shift(zkg_coset* c, zkg_buf* data) {
   return guard([&] {
     need(c, "coset");
     need(data, "data");
+    wait_reads(data, c->shift.ctx->stream);
     c->shift.run(data);
     mark_use(data, c->shift.ctx->stream);
   });
@@ -563,6 +582,7 @@ int zkg_ntt_inverse_coset(zkg_ntt* ntt, zkg_buf* data, zkg_coset* c) {
     need(ntt, "ntt");
     need(data, "data");
     need(c, "coset");
+    wait_reads(data, ntt->plan.ctx->stream);
     ntt->plan.run(data, true, &c->shift);
     mark_use(data, ntt->plan.ctx->stream);
   });
@@ -736,7 +756,10 @@ int zkg_tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int reps, int* bes
   return guard([&] {
     need(ctx, "ctx");
     need(data, "data");
+    use(ctx);
+    wait_reads(data, ctx->stream);
     auto all = tune_ntt(ctx, log_n, data, reps < 1 ? 1 : reps);
+    mark_use(data, ctx->stream);
     if (all.empty()) fail(ZKG_EINVAL, "no pass split applies to this size");
     if (best_variant) *best_variant = all[0].variant;
     if (best_max_stages) *best_max_stages = all[0].max_stages;
@@ -760,7 +783,11 @@ int zkg_generator_multiples(zkg_ctx* ctx, int group, const zkg_buf* scalars, siz
     need(scalars, "scalars");
     need(out, "out");
     if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+    use(ctx);
+    wait_reads(out, ctx->stream);
     if (n) generator_multiples(ctx, group, scalars, n, mont256, out);
+    mark_use(out, ctx->stream);
+    mark_use(scalars, ctx->stream);
   });
 }
 

@@ -56,6 +56,7 @@ struct MsmPlan {
   MsmPlan(zkg_ctx* ctx, int group, size_t n, uint32_t c, uint32_t item_points);
   ~MsmPlan() {
     if (result_handle.last_use) cudaEventDestroy(result_handle.last_use);
+    if (result_handle.pending_read) cudaEventDestroy(result_handle.pending_read);
   }
   MsmPlan(const MsmPlan&) = delete;
   MsmPlan& operator=(const MsmPlan&) = delete;

@@ -70,9 +70,13 @@ struct zkg_buf {
   uint32_t* ptr = nullptr;
   size_t words = 0;
   bool owned = true;  // false for plan-owned results handed out as borrowed handles
-  // Recorded after the last queued work that uses the buffer (a kernel on the context stream
-  // or an asynchronous read): an asynchronous write waits for it (created on first use).
+  // Recorded after the last queued work that uses the buffer (a kernel on the context stream,
+  // an asynchronous read or write): an asynchronous write waits for it, and so does an
+  // asynchronous read (the data's producer is the last use before it). Created on first use.
   cudaEvent_t last_use = nullptr;
+  // Recorded after the last asynchronous read: work that writes the buffer waits for it, other
+  // work does not (a read-back overlaps the kernels queued after it).
+  cudaEvent_t pending_read = nullptr;
 };
 
 namespace zkg {
@@ -86,6 +90,11 @@ inline void mark_use(const zkg_buf* b, cudaStream_t stream) {
   zkg_buf* m = const_cast<zkg_buf*>(b);
   if (!m->last_use) check_cuda(cudaEventCreateWithFlags(&m->last_use, cudaEventDisableTiming), "cudaEventCreate");
   check_cuda(cudaEventRecord(m->last_use, stream), "cudaEventRecord");
+}
+
+// Work about to be queued on `stream` writes `b`: it waits for the queued asynchronous reads of b.
+inline void wait_reads(const zkg_buf* b, cudaStream_t stream) {
+  if (b && b->pending_read) check_cuda(cudaStreamWaitEvent(stream, b->pending_read, 0), "cudaStreamWaitEvent");
 }
 
 inline uint32_t* device_alloc(size_t bytes, const char* what) {
