@@ -40,10 +40,12 @@ FP64_PER_MULMOD = 170  # double-precision instructions per Fq product in limb fo
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
 # ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured at 2^22
 # (profiles/msm_accumulate_f64_g1_2^22.md, 7.05 GB) and scaled by the entry count to 2^24 (x4);
-# ntt_pass: captured at 2^24 (profiles/ntt_pass_2^24.md).
+# ntt_pass / ntt_pass_f64: first pass captured at 2^24 (profiles/ntt_pass_2^24.md,
+# profiles/ntt_pass_f64_2^24.md).
 NCU_TRAFFIC = {
     "msm_accumulate_2^24": 28.2e9,
     "ntt_pass_2^24": 1.96e9,
+    "ntt_pass_f64_2^24": 2.18e9,
 }
 
 
@@ -390,14 +392,15 @@ def run_ours(a, d: Dist) -> dict | None:
                           "algorithmic": f"{FP64_PER_MULMOD} FP64 instructions per Fq product"},
         },
         "roofline_ntt": {
-            "kernel": f"ntt_pass (Fr NTT 2^{a.log_ntt}, {n_pass} passes)",
+            "kernel": (f"ntt_pass_f64 (Fr NTT 2^{a.log_ntt}, {n_pass} passes; butterflies in FP64 limbs)"
+                       if ntt.params()["variant"] == 1 else f"ntt_pass (Fr NTT 2^{a.log_ntt}, {n_pass} passes)"),
             "bound": "hbm",
             "achieved": round(ntt_gbs, 1),
             "peak": hbm_peak,
             "unit": "GB/s",
             "frac": round(ntt_gbs / hbm_peak, 4),
             "peak_source": hbm_src,
-            "traffic": NCU_TRAFFIC["ntt_pass_2^24"],
+            "traffic": NCU_TRAFFIC["ntt_pass_f64_2^24" if ntt.params()["variant"] == 1 else "ntt_pass_2^24"],
             "algorithmic": "64 B per element per pass (read + write)",
             "transform_frac_of_hbm": round((ntt_bytes * n_pass / (sum(stn.values()) * 1e-3) / 1e9) / hbm_peak, 4),
         },
@@ -467,12 +470,12 @@ def run_serving(a, gpu) -> dict:
         for n, g1, g2 in keys:
             sv.add_key(n, g1, g2)
         # warm every size class once (slot creation, graph capture) outside the timing; the
-        # served mode runs several requests of one size at once, so it keeps two slots per size
+        # served mode runs several requests of one size at once, so it keeps three slots per size
         # ready (more are made on its builder thread when a stream needs them)
         for k in sorted(pool):
             sv.wait(sv.submit(pool[k]))
             if mode == "batched":
-                sv.reserve(k, 2)
+                sv.reserve(k, 3)
         servers[mode] = sv
     for rate in rates:
         rng = np.random.default_rng(int(rate * 1000) + 17)

@@ -72,8 +72,8 @@ def test_tuning_knobs_reject_out_of_range_values(gpu):
     ntt = Ntt(gpu, 12)
     with pytest.raises(ZkGpuError, match="NTT variant must be 0 or 1"):
         ntt.set_variant(2)
-    with pytest.raises(ZkGpuError, match=r"max_stages must be in 6..=11"):
-        ntt.set_max_stages(12)
-    ntt.set_variant(1)
     with pytest.raises(ZkGpuError, match=r"max_stages must be in 6..=10"):
         ntt.set_max_stages(11)
+    ntt.set_variant(0)
+    with pytest.raises(ZkGpuError, match=r"max_stages must be in 6..=11"):
+        ntt.set_max_stages(12)

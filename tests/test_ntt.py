@@ -24,13 +24,14 @@ def test_matches_oracle(gpu, log_n):
 
 
 @pytest.mark.parametrize("log_n", [10, 11, 13, 16, 20])
-def test_double_precision_form_matches_oracle(gpu, log_n):
-    """The double-precision butterfly form (variant 1) beside the default integer one."""
+def test_integer_form_matches_oracle(gpu, log_n):
+    """The integer butterfly form (variant 0) beside the default double-precision one (which
+    every other test of this file runs)."""
     x = random_fr(300 + log_n, 1 << log_n)
     ntt = Ntt(gpu, log_n)
-    assert ntt.params()["variant"] == 0
-    ntt.set_variant(1)
     assert ntt.params()["variant"] == 1
+    ntt.set_variant(0)
+    assert ntt.params()["variant"] == 0
     assert np.array_equal(gpu_ntt(gpu, ntt, x), cpu.ntt(x)), f"log_n={log_n}"
     assert np.array_equal(gpu_ntt(gpu, ntt, cpu.ntt(x), inverse=True), x), f"log_n={log_n}"
 

@@ -165,10 +165,13 @@ __device__ __forceinline__ Fr fr_from_limbs(const f64::FqD& v) {
 
 // ntt_pass with double-precision butterflies; tw holds 5 doubles per twiddle, the tile is stored
 // limb-major (limb k of slot e at k * elems + e) so consecutive threads touch consecutive doubles.
+// Three blocks of 256 threads per SM (80 registers): with two (116 registers) the warps stalled
+// on the twiddle loads (2^24: 5.97 -> 5.32 ms per transform; four blocks spill, 5.40 ms).
 template <bool LAST>
-__global__ void __launch_bounds__(kNttThreads, 2)
+__global__ void __launch_bounds__(kNttThreads, 3)
     ntt_pass_f64(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const double* __restrict__ tw,
-                 uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale_mont) {
+                 uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag, Fr scale_mont,
+                 const uint32_t* __restrict__ sh_hi, const uint32_t* __restrict__ sh_lo, uint32_t sh_bits) {
   using namespace f64;
   extern __shared__ __align__(16) double tile_d[];
   const MultiplesOf<FrLimbs>* kr = &g_multiples_of_r;
@@ -220,8 +223,9 @@ __global__ void __launch_bounds__(kNttThreads, 2)
     __syncthreads();
   }
 
+  const bool shifted = LAST && sh_hi != nullptr;  // the coset shift (with 1/n) as in ntt_pass
   FqD scale;
-  if (scale_flag) {
+  if (scale_flag && !shifted) {
     uint32_t w[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) w[i] = scale_mont.w[i];
@@ -229,10 +233,16 @@ __global__ void __launch_bounds__(kNttThreads, 2)
   }
   for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
     FqD v = tile_load_d(tile_d, elems, slot);
-    if (scale_flag) v = fqd_mul<FrLimbs>(v, scale);
+    if (scale_flag && !shifted) v = fqd_mul<FrLimbs>(v, scale);
     uint32_t g = tile_global_index(tile, slot, lg, lm, s);
     if (LAST) g = __brev(g) >> (32 - log_n);
-    store_fe(dst + 8 * (size_t)g, fr_from_limbs(v));
+    Fr out = fr_from_limbs(v);
+    if (shifted) {
+      const Fr gi = load_fe<Fr>(sh_hi + 8 * (size_t)(g >> sh_bits)) *
+                    load_fe<Fr>(sh_lo + 8 * (size_t)(g & ((1u << sh_bits) - 1)));
+      out = out * gi;
+    }
+    store_fe(dst + 8 * (size_t)g, out);
   }
 }
 
@@ -268,7 +278,9 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
              "ntt smem attribute");
   check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "ntt smem attribute");
-  set_variant(0);
+  // Double-precision butterflies by default: on B200 they are 40% faster up to 2^17 elements
+  // (smaller tiles, more blocks), 13% at 2^20 and within 1% from 2^21 to 2^24.
+  set_variant(1);
 }
 
 uint32_t NttPlan::tile_log() const { return variant == 1 ? kTileLogD : kTileLog; }
@@ -360,17 +372,10 @@ const NttPlan::FusedShift* NttPlan::fused_for(const CosetShift& shift) {
   return fused.back().get();
 }
 
-void NttPlan::prepare_shift(const CosetShift& shift) {
-  if (variant == 0) fused_for(shift);
-}
+void NttPlan::prepare_shift(const CosetShift& shift) { fused_for(shift); }
 
 void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift) {
   if (shift && !inverse) fail(ZKG_EINVAL, "a fused coset shift follows an inverse transform");
-  if (shift && variant == 1) {  // double-precision form: the shift as its own kernel
-    enqueue(data, inverse, s);
-    const_cast<CosetShift*>(shift)->enqueue(data, s);
-    return;
-  }
   const FusedShift* fs = shift ? fused_for(*shift) : nullptr;
   const uint32_t* sh_hi = fs ? shift->hi.ptr : nullptr;
   const uint32_t* sh_lo = fs ? fs->lo.ptr : nullptr;
@@ -394,9 +399,11 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
     const int scale_flag = last && inverse;
     size_t ev = timer.enabled ? timer.begin((int)i, s) : 0;
     if (variant == 1 && last)
-      ntt_pass_f64<true><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass_f64<true><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale, sh_hi,
+                                                          sh_lo, sh_bits);
     else if (variant == 1)
-      ntt_pass_f64<false><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale);
+      ntt_pass_f64<false><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale,
+                                                           nullptr, nullptr, 0);
     else if (last)
       ntt_pass<true><<<tiles, kNttThreads, smem, s>>>(src, dst, tw, log_n, tl, lm, st, scale_flag, scale, sh_hi,
                                                       sh_lo, sh_bits);

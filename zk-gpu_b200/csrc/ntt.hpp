@@ -24,16 +24,17 @@ struct NttPlan {
   StageTimer timer;  // one stage id per pass
 
   NttPlan(zkg_ctx* ctx, uint32_t log_n);
-  // Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs (measured
-  // 12% slower at 2^24 on B200; the tuner may still pick it). Resets the pass split to the
+  // Butterfly form: 0 = 32-bit integer products, 1 = double-precision limbs (the default; on
+  // B200 40% faster than form 0 up to 2^17 elements, 13% at 2^20, within 1% from 2^21 to 2^24;
+  // the tuner times both). Resets the pass split to the
   // form's default. The first switch to form 1 builds its twiddle limbs (set-up stream, waited for).
   bool set_variant(int variant);
-  int variant = 0;
+  int variant = 1;
   uint32_t tile_log() const;
   // Splits the stages into passes of at most max_stages (6..tile_log()); false if not applicable
   // (transforms of one tile have a single pass).
   bool set_max_stages(uint32_t max_stages);
-  uint32_t max_stages = 9;
+  uint32_t max_stages = 8;
   // Queues one transform of data (2^log_n elements) on stream s. With `shift` (inverse only),
   // the coset shift x_i <- x_i * g^i of that object is applied in the transform's last pass
   // (the same result as the transform followed by shift->enqueue, without another pass over

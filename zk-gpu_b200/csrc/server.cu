@@ -103,7 +103,7 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
     const size_t heads = entries / L + 1;
     return 4 * (3 * S + entries + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
   };
-  const size_t ntt = 32 * N + 2 * 16 * N;
+  const size_t ntt = 32 * N + 2 * 16 * N + 2 * 20 * N;  // scratch, twiddle words and limbs
   const size_t bufs = 3 * 32 * m + 32 * m + 3 * 32 * N + 4096;
   return msm(32) + msm(64) + ntt + bufs;
 }
