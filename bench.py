@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -122,7 +123,9 @@ class ClockSampler:
         ids = [v.strip() for v in vis.split(",") if v.strip()]
         self.target = ids[local_rank] if local_rank < len(ids) else str(local_rank)
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{local_rank}.csv")
+        # the raw samples (the JSON line carries their summary); ZKG_CLOCK_LOG_DIR chooses where
+        log_dir = os.environ.get("ZKG_CLOCK_LOG_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(log_dir, f"clocks_rank{local_rank}.csv")
 
     def start(self):
         try:

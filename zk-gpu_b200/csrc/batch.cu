@@ -1,6 +1,6 @@
 // Batched execution: many MSMs, NTTs and coset shifts of uneven sizes captured into one CUDA
-// graph and replayed with a single launch (SURVEY a'2; the plain form is one Msm::run /
-// Ntt::forward per call, src/msm.rs:286, src/ntt.rs:52).
+// graph and replayed with a single launch (the plain form is one Msm::run / Ntt::forward per
+// call, src/msm.rs:286, src/ntt.rs:52).
 //
 // Operations are recorded on "lanes". Operations in one lane run in order; different lanes
 // are independent graph branches, so the device overlaps them (a lane per request lets the

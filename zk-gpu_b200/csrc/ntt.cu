@@ -434,8 +434,8 @@ namespace zkg {
 // ------------------------------------------------------------------ coset shift
 //
 // x_i <- x_i * g^i for i < n (the distribute-powers step between the inverse and forward
-// transforms of a Groth16 witness map; SURVEY a'1, README.md:229-230 of the reference names it
-// as a kernel on top). g^i = hi[i >> lo_bits] * lo[i & mask] from two small tables of powers, so
+// transforms of a Groth16 witness map; README.md:229-230 of the reference names it as a kernel
+// on top). g^i = hi[i >> lo_bits] * lo[i & mask] from two small tables of powers, so
 // each element costs two Fr products and one read and write of 32 bytes.
 __global__ void coset_shift_kernel(uint32_t* __restrict__ data, size_t n, const uint32_t* __restrict__ hi,
                                    const uint32_t* __restrict__ lo, uint32_t lo_bits) {

@@ -1,6 +1,5 @@
-// Proving-request server: the serving form of the hot path (SURVEY a'4; the reference has no
-// server, its callers issue one Msm::run / Ntt::forward at a time, src/msm.rs:286,
-// src/ntt.rs:43-50).
+// Proving-request server: the serving form of the hot path (the reference has no server, its
+// callers issue one Msm::run / Ntt::forward at a time, src/msm.rs:286, src/ntt.rs:43-50).
 //
 // A request is Groth16-shaped: three G1 MSMs (sizes m, m, m - 1024) and one G2 MSM (size m) over
 // the smallest resident proving key with at least m points, and a witness-map chain of seven

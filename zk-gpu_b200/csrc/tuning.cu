@@ -1,4 +1,4 @@
-// Autotuner (SURVEY a'3): measures candidate launch parameters on the device and returns the
+// Autotuner: measures candidate launch parameters on the device and returns the
 // fastest. The reference fixes its parameters (Msm::default_window, src/msm.rs:78-80; item size
 // mean_bucket/4, :99-100; TILE_LOG = 9 for the NTT, src/ntt.rs:9) and sweeps windows by hand
 // (examples/g2_window.rs:50-69); default_window stays the plain form beside the tuned one.
