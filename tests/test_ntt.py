@@ -232,3 +232,17 @@ def test_every_pass_split_is_exact(gpu, tmp_path, monkeypatch):
     buf = gpu.buffer(x)
     ntt = tuned_ntt(gpu, log_n, buf, reps=1)
     assert np.array_equal(gpu_ntt(gpu, ntt, x), want)
+
+
+def test_plans_of_different_sizes_interleave(gpu):
+    """A small plan made after a large one does not shrink what the large one's passes may use
+    (a per-kernel launch limit): both forms, run in turn."""
+    big_x, small_x = random_fr(600, 1 << 16), random_fr(601, 1 << 10)
+    big = Ntt(gpu, 16)
+    small = Ntt(gpu, 10)
+    for variant in (0, 1, 0):
+        big.set_variant(variant)
+        small.set_variant(variant)
+        assert np.array_equal(gpu_ntt(gpu, big, big_x), cpu.ntt(big_x)), f"variant {variant}"
+        assert np.array_equal(gpu_ntt(gpu, small, small_x), cpu.ntt(small_x)), f"variant {variant}"
+        Ntt(gpu, 10)  # another small plan between runs

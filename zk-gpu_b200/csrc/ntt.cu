@@ -167,6 +167,8 @@ __device__ __forceinline__ Fr fr_from_limbs(const f64::FqD& v) {
 // limb-major (limb k of slot e at k * elems + e) so consecutive threads touch consecutive doubles.
 // Three blocks of 256 threads per SM (80 registers): with two (116 registers) the warps stalled
 // on the twiddle loads (2^24: 5.97 -> 5.32 ms per transform; four blocks spill, 5.40 ms).
+// Copying each thread's next-stage twiddles into shared memory with 8-byte cp.async (60 KiB per
+// block) made it slower still: 6.49 ms.
 template <bool LAST>
 __global__ void __launch_bounds__(kNttThreads, 3)
     ntt_pass_f64(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const double* __restrict__ tw,
@@ -257,6 +259,17 @@ static std::vector<uint32_t> powers_words(const host::U256& step, size_t len) {
   return out;
 }
 
+// The largest dynamic shared memory a pass launch asks for (a function attribute: one value for
+// every plan on the device, so always the largest tile's; the double-precision tiles, 40 KiB,
+// stay under the 48 KiB that needs no attribute).
+static void set_pass_smem_limits() {
+  const int smem = (int)((size_t)32 << kTileLog);
+  check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+             "ntt smem attribute");
+}
+
 NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   if (log_n < 10 || log_n > 27) fail(ZKG_EINVAL, "log_n must be in 10..=27");
   use(ctx);
@@ -273,11 +286,7 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   build_twiddles(w_inv, inv_tw, seeds[1]);
   // Set-up work runs on the set-up stream: done before the plan is used on any stream.
   check_cuda(cudaStreamSynchronize(ctx->setup), "ntt twiddles");
-  const size_t smem = (size_t)32 << (log_n < kTileLog ? log_n : kTileLog);
-  check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "ntt smem attribute");
-  check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "ntt smem attribute");
+  set_pass_smem_limits();
   // Double-precision butterflies by default: on B200 they are 40% faster up to 2^17 elements
   // (smaller tiles, more blocks), 13% at 2^20 and within 1% from 2^21 to 2^24.
   set_variant(1);
@@ -553,11 +562,7 @@ static uint32_t* noalloc_scratch(int device) {
   if (!g_noalloc_ptr[device]) {
     void* p = nullptr;
     check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
-    const int smem = (int)((size_t)32 << kTileLog);
-    check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-               "ntt smem attribute");
-    check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-               "ntt smem attribute");
+    set_pass_smem_limits();
     g_noalloc_ptr[device] = static_cast<uint32_t*>(p);
   }
   return g_noalloc_ptr[device];
