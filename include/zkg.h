@@ -126,9 +126,9 @@ int zkg_msm_group(const zkg_msm *msm);
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
 /* Counting-sort knob (no reference counterpart): how a warp merges the counting pass's atomics
- * for lanes whose digits hit the same (window, bucket) slot: 0 = every group of equal slots
- * (default), 1 = the group of the first lane only, 2 = none, 3 = the group of the first pair of
- * neighbouring lanes with equal slots. The scatter pass always merges every group. */
+ * for lanes whose digits hit the same (window, bucket) slot: 0 = every group of equal slots,
+ * 1 = the group of the first lane only, 2 = none, 3 = the group of the first pair of
+ * neighbouring lanes with equal slots (default). The scatter pass always merges every group. */
 int zkg_msm_set_sort(zkg_msm *msm, int mode);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32

@@ -137,6 +137,9 @@ __global__ void msm_count(const uint32_t* __restrict__ scalars, size_t n, uint32
 
 // Pass 3: scatter point indices (sign in bit 31) into slot order. Within a slot the order is
 // whatever the atomics give; bucket sums are exact, so the result does not depend on it.
+// Issuing 4 or 8 windows' atomics together measured 1-3% slower at 2^24, so the pass is not
+// bound by the atomics' round trips; its scattered 4-byte stores (a 32-byte sector each) are
+// the likely bound.
 template <int AGG>
 __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
                             uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
