@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--log-ntt", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched-vs-plain request stream")
-    ap.add_argument("--serving-rates", default="2,20,60,200", help="Poisson arrival rates (req/s)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the per-configuration timings")
+    ap.add_argument("--serving-rates", default="1,20,60,200", help="Poisson arrival rates (req/s)")
     ap.add_argument("--serving-lanes", type=int, default=8)
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small profiling case (Fq product probe, G1 MSM 2^22, Fr NTT 2^24 forward) and exit")
@@ -423,6 +424,8 @@ def run_ours(a, d: Dist) -> dict | None:
         "clocks": clk,
         "bit_exact": {"ntt_round_trip": round_trip, "e2e_round_trip": e2e_ok},
     }
+    if not a.no_configs:
+        out["configs"] = run_configs(gpu, bases, stream, n24)
     if not a.no_serving:
         out["serving"] = run_serving(a, gpu)
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
@@ -437,6 +440,72 @@ def run_ours(a, d: Dist) -> dict | None:
 
 SERVING_KEYS = (18, 20, 21, 22)  # resident proving keys, log2 of their sizes
 SERVING_K = (14, 22)             # circuit size m = 2^k, k uniform over these integers
+
+
+def run_configs(gpu, bases, stream, n_max) -> dict:
+    """Device time of one call at the other sizes of the benchmark configurations (outside the
+    timed step; inputs resident; CUDA events on the library stream, best of three after a
+    warm-up): G1 MSM 2^16..2^24 with default_window (uniform scalars, and the two skewed
+    distributions at 2^24), G2 MSM 2^18..2^22 (Montgomery-2^256 upload), Fr NTT 2^16..2^26."""
+    import torch
+
+    from zk_gpu import Group, Msm, Ntt
+    from zk_gpu.synthetic import generator_multiples, scalar_distribution, uniform_scalars
+
+    def device_ms(fn):
+        fn()
+        best = float("inf")
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return round(best, 3)
+
+    out = {"method": "device time of one call, best of 3 after a warm-up; inputs resident in HBM; NTT hbm_gbs = "
+                     "64 B per element per pass over the forward transform's time"}
+    g1 = {}
+    for lg in (16, 18, 20, 22, 24):
+        n = 1 << lg
+        if n > n_max:
+            continue
+        s = gpu.buffer(uniform_scalars(n, 300 + lg))
+        msm = Msm(gpu, n, Msm.default_window(n))
+        g1[f"2^{lg}"] = device_ms(lambda: msm.run(gpu, bases, s))  # the first n points of the key
+        if lg == 24:
+            for kind, seed in (("sparse", 1), ("r-1", 2)):
+                sk = gpu.buffer(scalar_distribution(n, kind, 400 + seed))
+                g1[f"2^{lg} {kind}"] = device_ms(lambda: msm.run(gpu, bases, sk))
+                sk.free()
+        msm.close()
+        s.free()
+    out["g1_msm_ms"] = g1
+    g2 = {}
+    n2 = 1 << 22
+    b2 = generator_multiples(gpu, Group.G2, uniform_scalars(n2, 500), mont256=True)
+    for lg in (18, 20, 22):
+        n = 1 << lg
+        s = gpu.buffer(uniform_scalars(n, 510 + lg))
+        msm = Msm.for_group(gpu, Group.G2, n, Msm.default_window(n))
+        g2[f"2^{lg}"] = device_ms(lambda: msm.run(gpu, b2, s))
+        msm.close()
+        s.free()
+    b2.free()
+    out["g2_msm_ms"] = g2
+    nt = {}
+    for lg in (16, 20, 22, 24, 26):
+        x = gpu.buffer(uniform_scalars(1 << lg, 600 + lg))
+        ntt = Ntt(gpu, lg)
+        fwd = device_ms(lambda: ntt.forward(gpu, x))
+        inv = device_ms(lambda: ntt.inverse(gpu, x))
+        nt[f"2^{lg}"] = {"forward": fwd, "inverse": inv, "passes": ntt.params()["passes"],
+                         "hbm_gbs": round(64 * (1 << lg) * ntt.params()["passes"] / (fwd * 1e-3) / 1e9, 1)}
+        ntt.close()
+        x.free()
+    out["ntt_ms"] = nt
+    return out
 
 
 def run_serving(a, gpu) -> dict:

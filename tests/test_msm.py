@@ -252,9 +252,10 @@ def test_fuzz(gpu):
 
 # ---------------------------------------------------------------- full sizes
 
-def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None):
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False):
     """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
-    uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G."""
+    uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G. tuned: the plan
+    (window, points per thread, form) comes from the autotuner on these inputs."""
     n = 1 << log_n
     k = uniform_scalars(n, 1000 + log_n + seed).reshape(n, 8)
     k[infinity_mask(n, inf_fraction, log_n + seed)] = 0
@@ -264,11 +265,16 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant
     dev.free()
     s = scalar_distribution(n, kind, 2000 + log_n + seed)
     c = c or Msm.default_window(n)
-    base_buf = Msm.upload_bases(gpu, plain)
-    msm = Msm(gpu, n, c)
-    if variant is not None:
-        msm.set_variant(variant)
-    got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, gpu.buffer(s)), 32)))
+    base_buf, scalar_buf = Msm.upload_bases(gpu, plain), gpu.buffer(s)
+    if tuned:
+        from zk_gpu.autotune import tuned_msm
+        msm = tuned_msm(gpu, Group.G1, n, base_buf, scalar_buf, reps=1)
+        c, variant = msm.params()["c"], msm.params()["variant"]
+    else:
+        msm = Msm(gpu, n, c)
+        if variant is not None:
+            msm.set_variant(variant)
+    got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, scalar_buf), 32)))
     gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
     want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
     assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}, variant = {variant}) wrong"
@@ -286,6 +292,14 @@ def test_full_size_distributions(gpu, log_n, kind):
 @pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"] if not quick() else ["uniform"])
 def test_full_size_2_24(gpu, kind):
     full_size_case(gpu, 24, kind)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"])
+@pytest.mark.parametrize("log_n", [18, 20, 22])
+def test_full_size_autotuned(gpu, log_n, kind, tmp_path, monkeypatch):
+    """The same cases with the autotuned window, points per thread and form."""
+    monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
+    full_size_case(gpu, log_n, kind, tuned=True)
 
 
 def test_full_size_other_window(gpu):
