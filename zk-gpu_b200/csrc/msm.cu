@@ -18,6 +18,24 @@
 
 namespace zkg {
 
+// Dynamic shared memory of msm_accumulate_f64: the G2 form keeps its accumulators there
+// (4 coordinates x 10 doubles x 128 threads); G1 keeps them in registers.
+template <class E>
+static size_t f64_acc_smem() {
+  return std::is_same<E, f64::Fq2D>::value ? (size_t)4 * f64::AccSmem<E>::N * 128 * sizeof(double) : 0;
+}
+
+// Allows the G2 form's dynamic shared memory beside its static staging buffers (72 KiB a block).
+static void set_acc_smem_limits() {
+  const int bytes = (int)f64_acc_smem<f64::Fq2D>();
+  check_cuda(cudaFuncSetAttribute(msm_accumulate_f64<f64::Fq2D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  bytes),
+             "accumulation smem attribute");
+  check_cuda(cudaFuncSetAttribute(msm_accumulate_f64<f64::Fq2D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  bytes),
+             "accumulation smem attribute");
+}
+
 uint32_t default_window(size_t n) {
   // clamp(log2(max(n,1)) - 5, 11, 16) (src/msm.rs:78-80)
   size_t v = n < 1 ? 1 : n;
@@ -56,6 +74,7 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
 
   use(ctx);
+  if (group == ZKG_G2) set_acc_smem_limits();
   counts.alloc(slots, "msm counts");
   slot_start.alloc(slots + 1, "msm slot_start");
   cursor.alloc(slots, "msm cursor");
@@ -163,11 +182,12 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
     case kStageAccumulate:
       if (acc_variant == 3 || acc_variant == 4) {
         using E = typename std::conditional<std::is_same<F, Fq>::value, f64::FqD, f64::Fq2D>::type;
+        const size_t acc_smem = f64_acc_smem<E>();
         if (acc_variant == 3)
-          msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, 0, s>>>(
+          msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
               bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else
-          msm_accumulate_f64<E, false><<<grid_for(heads_max, 128), 128, 0, s>>>(
+          msm_accumulate_f64<E, false><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
               bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       }
       else if (acc_variant == 1)

@@ -201,28 +201,84 @@ __device__ __forceinline__ bool xyzzd_double_slow(XyzzT<E>& acc, const Multiples
   return true;
 }
 
+// Where a thread's bucket accumulator lives. AccRegs: registers (G1). AccSmem: the block's
+// shared memory, limb-major over its 128 threads (slot k of thread t at base[k * 128 + t]), each
+// coordinate read right before it is used, so the addition's registers hold only its
+// temporaries (a G2 accumulator is 40 doubles, which in registers push the kernel into spills).
+template <class E>
+struct AccRegs {
+  XyzzT<E> v;
+  __device__ __forceinline__ E x() const { return v.x; }
+  __device__ __forceinline__ E y() const { return v.y; }
+  __device__ __forceinline__ E zz() const { return v.zz; }
+  __device__ __forceinline__ E zzz() const { return v.zzz; }
+  __device__ __forceinline__ XyzzT<E> get() const { return v; }
+  __device__ __forceinline__ void set(const XyzzT<E>& a) { v = a; }
+};
+__device__ __forceinline__ void slots_ld(const double* p, FqD& e) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) e.l[k] = p[k * 128];
+}
+__device__ __forceinline__ void slots_ld(const double* p, Fq2D& e) {
+  slots_ld(p, e.a);
+  slots_ld(p + 5 * 128, e.b);
+}
+__device__ __forceinline__ void slots_st(double* p, const FqD& e) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) p[k * 128] = e.l[k];
+}
+__device__ __forceinline__ void slots_st(double* p, const Fq2D& e) {
+  slots_st(p, e.a);
+  slots_st(p + 5 * 128, e.b);
+}
+template <class E>
+struct AccSmem {
+  static constexpr int N = sizeof(E) / sizeof(double);  // doubles per element
+  double* base;  // &slots[threadIdx.x]
+  __device__ __forceinline__ E ld(int coord) const {
+    E e;
+    slots_ld(base + coord * N * 128, e);
+    return e;
+  }
+  __device__ __forceinline__ void st(int coord, const E& e) { slots_st(base + coord * N * 128, e); }
+  __device__ __forceinline__ E x() const { return ld(0); }
+  __device__ __forceinline__ E y() const { return ld(1); }
+  __device__ __forceinline__ E zz() const { return ld(2); }
+  __device__ __forceinline__ E zzz() const { return ld(3); }
+  __device__ __forceinline__ XyzzT<E> get() const { return XyzzT<E>{ld(0), ld(1), ld(2), ld(3)}; }
+  __device__ __forceinline__ void set(const XyzzT<E>& a) {
+    st(0, a.x);
+    st(1, a.y);
+    st(2, a.zz);
+    st(3, a.zzz);
+  }
+};
+
 // acc += (bx, by) with acc not at infinity (madd-2008-s), with the bounds stated at the top of
 // this file. Returns false when the sum is infinity.
-template <class E, bool PAIRS>
-__device__ __forceinline__ bool xyzzd_add_affine(XyzzT<E>& acc, const E& bx, const E& by, const MultiplesOfP* kp) {
+template <class E, bool PAIRS, class Acc>
+__device__ __forceinline__ bool xyzzd_add_affine(Acc& acc, const E& bx, const E& by, const MultiplesOfP* kp) {
   E u2, s2;
-  e_mul2<PAIRS>(bx, acc.zz, by, acc.zzz, u2, s2, kp);
-  const E pp = e_sub<2>(u2, acc.x);
-  const E r = e_sub<2>(s2, acc.y);
+  e_mul2<PAIRS>(bx, acc.zz(), by, acc.zzz(), u2, s2, kp);
+  const E pp = e_sub<2>(u2, acc.x());
+  const E r = e_sub<2>(s2, acc.y());
   if (e_is_zero4(pp)) {
     if (!e_is_zero4(r)) return false;
-    return xyzzd_double_slow(acc, kp);
+    XyzzT<E> t = acc.get();
+    const bool live = xyzzd_double_slow(t, kp);
+    if (live) acc.set(t);
+    return live;
   }
   E ppsq, rr, ppp, q;
   e_sqr2<PAIRS>(pp, r, ppsq, rr, kp);
-  e_mul2<PAIRS>(pp, ppsq, acc.x, ppsq, ppp, q, kp);
+  e_mul2<PAIRS>(pp, ppsq, acc.x(), ppsq, ppp, q, kp);
   const E d = e_add(q, q);
   const E x3 = e_reduce(e_sub2<6>(rr, ppp, d), kp);
   const E v = e_sub<2>(q, x3);
-  const E y3 = e_mul_sub<PAIRS>(r, v, acc.y, ppp, kp);  // R V - Y PPP
+  const E y3 = e_mul_sub<PAIRS>(r, v, acc.y(), ppp, kp);  // R V - Y PPP
   E zz3, zzz3;
-  e_mul2<PAIRS>(acc.zz, ppsq, acc.zzz, ppp, zz3, zzz3, kp);
-  acc = XyzzT<E>{x3, y3, zz3, zzz3};
+  e_mul2<PAIRS>(acc.zz(), ppsq, acc.zzz(), ppp, zz3, zzz3, kp);
+  acc.set(XyzzT<E>{x3, y3, zz3, zzz3});
   return true;
 }
 
@@ -232,10 +288,12 @@ __device__ __forceinline__ bool xyzzd_add_affine(XyzzT<E>& acc, const E& bx, con
 // FqD (G1) or Fq2D (G2); PAIRS: two products per out-of-line call, else one. The next base is
 // fetched into shared memory with cp.async (two slots per thread) while the current addition
 // runs, so the prefetch holds no registers (G1: 50.9 ms at 2^24 against 52.9 ms fetching into
-// registers). G2 limb buckets are 80 registers on their own: that kernel spills. Three blocks of
-// 128 threads per SM (168 registers) measured faster than four (128 registers and ~100 bytes of
-// spills per thread: 48.5 against 48.0 ms at 2^24).
-template <class E, bool PAIRS>
+// registers). Three blocks of 128 threads per SM (168 registers) measured faster than four (128
+// registers and ~100 bytes of spills per thread: 48.5 against 48.0 ms at 2^24). G2 keeps the
+// accumulators in shared memory (AccSmem; in registers they are 80 of them and the kernel
+// spilled): 55.9 / 63.0 ms at 2^22 for one / two products per call, from 67 / 73, still behind
+// the integer pairs (47.3 ms); at three blocks per SM it spills again.
+template <class E, bool PAIRS, bool SMEM_ACC = !std::is_same<E, f64::FqD>::value>
 __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? 3 : 2)
     msm_accumulate_f64(const uint32_t* __restrict__ bases, const uint32_t* __restrict__ sorted,
                        const uint32_t* __restrict__ slot_start, uint32_t num_slots, uint32_t seg_len,
@@ -259,7 +317,10 @@ __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? 3 : 2)
   bool head = __ldg(&slot_start[s]) < p0;
   uint32_t head_key = kNoKey;
 
-  XyzzT<E> acc;
+  using Acc = typename std::conditional<SMEM_ACC, AccSmem<E>, AccRegs<E>>::type;
+  extern __shared__ __align__(16) double acc_slots[];  // SMEM_ACC: 4 * AccSmem<E>::N * 128 doubles
+  Acc acc;
+  if constexpr (SMEM_ACC) acc.base = acc_slots + threadIdx.x;
   bool empty = true;
   __shared__ __align__(16) uint32_t stage[2][128][AW];
   auto stage_base = [&](uint32_t slot, uint32_t e) {  // x then y
@@ -287,11 +348,11 @@ __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? 3 : 2)
     slot ^= 1;
     if (p == end) {
       if (head) {
-        store_xyzzd(heads + (size_t)t * XW, acc, empty);
+        store_xyzzd(heads + (size_t)t * XW, acc.get(), empty);
         head_key = s;
         head = false;
       } else {
-        store_xyzzd(buckets + (size_t)s * XW, acc, empty);
+        store_xyzzd(buckets + (size_t)s * XW, acc.get(), empty);
       }
       empty = true;
       uint32_t s2 = s + 1;
@@ -302,17 +363,17 @@ __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? 3 : 2)
     if (is_infinity(cur)) continue;
     const E bx = e_base(cur.x, kp), by = e_base(cur.y, kp);
     if (empty) {
-      acc = XyzzT<E>{e_reduce(bx, kp), e_reduce(by, kp), e_one260<E>(), e_one260<E>()};
+      acc.set(XyzzT<E>{e_reduce(bx, kp), e_reduce(by, kp), e_one260<E>(), e_one260<E>()});
       empty = false;
     } else {
       empty = !xyzzd_add_affine<E, PAIRS>(acc, bx, by, kp);
     }
   }
   if (head) {
-    store_xyzzd(heads + (size_t)t * XW, acc, empty);
+    store_xyzzd(heads + (size_t)t * XW, acc.get(), empty);
     head_key = s;
   } else {
-    store_xyzzd(buckets + (size_t)s * XW, acc, empty);
+    store_xyzzd(buckets + (size_t)s * XW, acc.get(), empty);
   }
   head_keys[t] = head_key;
 }
