@@ -36,7 +36,7 @@ struct MsmPlan {
   // products per call / one. Every form fetches the next base into shared memory with
   // cp.async. Defaults (measured on B200): G1 3 below 2^26 (window, point) entries and 4 above
   // (2^24: 48.1 ms against 50.1 for 3 and 59.7 for 2; 2^20: 3.98 against 4.11 for 4), G2 2
-  // (47.4 ms at 2^22 against 48.1 for 1; the limb forms spill for G2). Tunable.
+  // (47.4 ms at 2^22 against 48.1 for 1 and 55.9 / 63.0 for the limb forms 4 / 3). Tunable.
   int acc_variant = 4;
   // Warp aggregation of the counting pass's atomics (slot_peers in msm_kernels.cuh): 0 = every
   // group of equal slots, 1 = the first lane's group, 2 = none, 3 = the group of the first equal
