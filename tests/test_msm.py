@@ -242,6 +242,45 @@ def fuzz_case(gpu, seed):
         f"scalars={scalar_kind}, bases={base_kind})")
 
 
+def fuzz_forms_case(gpu, seed):
+    """One random edge-heavy MSM (G1, or G2 one time in four) through accumulation forms 1-4."""
+    rnd = np.random.default_rng(seed)
+    g = "G2" if int(rnd.integers(0, 4)) == 0 else "G1"
+    group = Group.G2 if g == "G2" else Group.G1
+    n = int([rnd.integers(1, 64), rnd.integers(1, 1500), rnd.integers(1, 5000)][rnd.integers(0, 3)])
+    n = min(n, 1500) if g == "G2" else n
+    c = int(rnd.integers(9, 17))
+    item_points = int([1, 2, 5, 64, 1024][rnd.integers(0, 5)])
+    aw = group.affine_words()
+    pool = random_points(g, seed * 3 + 1, 4).reshape(4, aw)
+    bases = random_points(g, seed * 3 + 2, n).reshape(n, aw)
+    kind = int(rnd.integers(0, 3))
+    if kind == 1:
+        bases = pool[rnd.integers(0, 4, size=n)]  # repeats: doublings inside buckets
+    elif kind == 2:
+        bases = bases.copy()
+        bases[rnd.random(n) < 0.1] = 0  # points at infinity
+    sk = int(rnd.integers(0, 3))
+    if sk == 0:
+        s = random_fr(seed * 3 + 3, n)
+    elif sk == 1:
+        s = fr_words(int(v) for v in rnd.integers(0, 16, size=n))
+    else:
+        s = fr_words([0, 1, R - 1][int(v)] for v in rnd.integers(0, 3, size=n))
+    bases = np.ascontiguousarray(bases.reshape(-1))
+    want = msm_ref(g, bases, s)
+    for variant in (1, 2, 3, 4):
+        got = gpu_msm(gpu, bases, s, (c, item_points), group=group, variant=variant)
+        assert np.array_equal(got, want), (
+            f"seed {seed}: {g} n={n} c={c} item_points={item_points} bases={kind} scalars={sk} form {variant}")
+
+
+def test_fuzz_every_form(gpu):
+    """Every accumulation form on the same random edge-heavy inputs (G1 and G2)."""
+    for seed in range(5000, 5000 + (10 if quick() else 40)):
+        fuzz_forms_case(gpu, seed)
+
+
 def test_fuzz(gpu):
     if "ZK_GPU_FUZZ_SEED" in os.environ:
         return fuzz_case(gpu, int(os.environ["ZK_GPU_FUZZ_SEED"]))
