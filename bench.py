@@ -656,7 +656,8 @@ def run_reference(a, d: Dist) -> dict | None:
 
 def profile_case():
     """The small case the ncu captures in profiles/ run: one Fq product probe launch set, one
-    G1 MSM 2^22 (device-built bases, uniform scalars) and one Fr NTT 2^24 forward."""
+    G1 MSM 2^22 (device-built bases, uniform scalars), one Fr NTT 2^24 forward and one G2 MSM
+    2^20 (device-built bases, Montgomery-2^256 form, uniform scalars)."""
     from zk_gpu import Gpu, Group, Msm, Ntt, lib
     from zk_gpu._lib import check
     from zk_gpu.synthetic import generator_multiples, uniform_scalars
@@ -676,6 +677,14 @@ def profile_case():
     buf = gpu.buffer(uniform_scalars(1 << 24, 3))
     ntt = Ntt(gpu, 24)
     ntt.forward(gpu, buf)
+    gpu.wait()
+    ntt.close()
+    buf.free()
+    n2 = 1 << 20
+    bases2 = generator_multiples(gpu, Group.G2, uniform_scalars(n2, 4), mont256=True)
+    s2 = gpu.buffer(uniform_scalars(n2, 5))
+    msm2 = Msm.for_group(gpu, Group.G2, n2, Msm.default_window(n2))
+    msm2.run(gpu, bases2, s2)
     gpu.wait()
     print("profile case done", flush=True)
 
