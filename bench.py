@@ -424,9 +424,11 @@ def run_ours(a, d: Dist) -> dict | None:
         "clocks": clk,
         "bit_exact": {"ntt_round_trip": round_trip, "e2e_round_trip": e2e_ok},
     }
-    if not a.no_configs:
+    # the per-configuration timings and the request stream are single-GPU measurements: a scaling
+    # run (N > 1 replicas) reports the step alone and releases the GPUs sooner
+    if not a.no_configs and d.world == 1:
         out["configs"] = run_configs(gpu, bases, stream, n24)
-    if not a.no_serving:
+    if not a.no_serving and d.world == 1:
         out["serving"] = run_serving(a, gpu)
     if d.rank == 0 and d.world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"], checks = cpu_baseline(a, gpu, bases, k, s20_host, s24_host, x_host, res20, res24,
