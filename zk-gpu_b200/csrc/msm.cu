@@ -47,11 +47,14 @@ uint32_t default_window(size_t n) {
 }
 
 // Points accumulated per thread when the caller does not choose, by the number of (point,
-// window) entries; measured on B200 (G1, uniform scalars): 2^16 points best at 16, 2^20 at 64,
-// 2^24 at 128 (fewer, longer segments cost merge work; more, shorter ones cost heads).
+// window) entries; measured on B200 (G1, uniform scalars, sweeping 8..128): 2^14 points best at
+// 8, 2^16 at 16, 2^18 at 32, 2^20 at 64, 2^22 and 2^24 at 128 (longer segments lengthen the
+// accumulation chains, shorter ones add heads and merge levels).
 static uint32_t auto_seg_len(size_t n, uint32_t windows) {
   const double entries = (double)n * windows;
-  if (entries < (double)(1u << 22)) return 16;
+  if (entries < (double)(1u << 19)) return 8;
+  if (entries < (double)(1u << 21)) return 16;
+  if (entries < (double)(1u << 23)) return 32;
   if (entries < (double)(1u << 26)) return 64;
   return 128;
 }
