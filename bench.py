@@ -65,7 +65,12 @@ def parse():
     ap.add_argument("--serving-rates", default="1,20,60,200", help="Poisson arrival rates (req/s)")
     ap.add_argument("--serving-lanes", type=int, default=8)
     ap.add_argument("--profile-case", action="store_true",
-                    help="run the small profiling case (Fq product probe, G1 MSM 2^22, Fr NTT 2^24 forward) and exit")
+                    help="run the small profiling case (Fq product probe, G1 MSM 2^22, Fr NTT 2^24 forward, "
+                         "G2 MSM 2^20) and exit")
+    ap.add_argument("--msm-form", type=int, choices=[0, 1, 2, 3, 4], default=None,
+                    help="profiling case: G1 accumulation form (default: the plan's default)")
+    ap.add_argument("--ntt-form", type=int, choices=[0, 1], default=None,
+                    help="profiling case: NTT butterfly form (0 integer, 1 FP64; default: the plan's default)")
     return ap.parse_args()
 
 
@@ -656,7 +661,7 @@ def run_reference(a, d: Dist) -> dict | None:
     }
 
 
-def profile_case():
+def profile_case(msm_form=None, ntt_form=None):
     """The small case the ncu captures in profiles/ run: one Fq product probe launch set, one
     G1 MSM 2^22 (device-built bases, uniform scalars), one Fr NTT 2^24 forward and one G2 MSM
     2^20 (device-built bases, Montgomery-2^256 form, uniform scalars)."""
@@ -671,6 +676,8 @@ def profile_case():
     bases = generator_multiples(gpu, Group.G1, uniform_scalars(n, 1), mont256=True)
     s = gpu.buffer(uniform_scalars(n, 2))
     msm = Msm(gpu, n, Msm.default_window(n))
+    if msm_form is not None:
+        msm.set_variant(msm_form)
     msm.run(gpu, bases, s)
     gpu.wait()
     msm.close()
@@ -678,6 +685,8 @@ def profile_case():
     s.free()
     buf = gpu.buffer(uniform_scalars(1 << 24, 3))
     ntt = Ntt(gpu, 24)
+    if ntt_form is not None:
+        ntt.set_variant(ntt_form)
     ntt.forward(gpu, buf)
     gpu.wait()
     ntt.close()
@@ -694,7 +703,7 @@ def profile_case():
 def main():
     a = parse()
     if a.profile_case:
-        return profile_case()
+        return profile_case(a.msm_form, a.ntt_form)
     d = Dist(a.gpus)
     try:
         out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)
