@@ -39,10 +39,9 @@ METRIC = "MSM 2^20/2^24 & NTT 2^24 ms, bit-exact; batched vs plain req/s, p50/p9
 IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m), field.cuh
 FP64_PER_MULMOD = 170  # double-precision instructions per Fq product in limb form, field_f64.cuh
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
-# ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured at 2^22
-# (profiles/msm_accumulate_f64_g1_2^22.md, 7.05 GB) and scaled by the entry count to 2^24 (x4);
-# ntt_pass / ntt_pass_f64: first pass captured at 2^24 (profiles/ntt_pass_2^24.md,
-# profiles/ntt_pass_f64_2^24.md).
+# ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured on a G1 MSM of
+# 2^22 points (7.05 GB) and scaled by the entry count to 2^24 (x4); ntt_pass / ntt_pass_f64:
+# first pass captured on the 2^24 transform.
 NCU_TRAFFIC = {
     "msm_accumulate_2^24": 28.2e9,
     "ntt_pass_2^24": 1.96e9,
@@ -214,7 +213,7 @@ def run_ours(a, d: Dist) -> dict | None:
     round_trip = bool(np.array_equal(gpu.read(data, x_host.size), x_host))
     fwd_probe = gpu.buffer(x_host)
     ntt.forward(gpu, fwd_probe)
-    ntt_fwd = gpu.read(fwd_probe, 8 * 4)  # first four outputs, checked against the CPU below
+    ntt_fwd = gpu.read(fwd_probe, x_host.size)  # the whole forward output, checked against the CPU below
     del fwd_probe
     entries = ctypes.c_uint64()
     check(L.zkg_msm_last_entries(msm24.__dict__["_h"], ctypes.byref(entries)))
@@ -611,7 +610,7 @@ def cpu_baseline(a, gpu, bases, k, s20, s24, x, res20, res24, ntt_fwd):
     checks = {
         f"msm_2^{a.log_msm}_vs_cpu": bool(np.array_equal(r24, res24)),
         f"msm_2^{a.log_msm_small}_vs_cpu": bool(np.array_equal(r20, res20)),
-        f"ntt_2^{a.log_ntt}_vs_cpu": bool(np.array_equal(y[:32], ntt_fwd)),
+        f"ntt_2^{a.log_ntt}_vs_cpu": bool(np.array_equal(y, ntt_fwd)),  # all 2^log_ntt outputs
     }
     return {"value": round(total * 1e3, 1), "unit": "ms", "cores": threads, "kind": "port",
             "sample": "one full step (both MSMs and the NTT pair) on the oracle's C restatement of the "

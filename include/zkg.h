@@ -294,7 +294,8 @@ int zkg_server_reserve(zkg_server *server, uint32_t log_m, uint32_t count);
  * process exits. Work is queued on `stream` (a cudaStream_t; NULL = the legacy default stream)
  * of the calling thread's current device. The first call on a device also resolves the array's
  * address for that device (cudaGetSymbolAddress) and sets the kernels' shared-memory limit;
- * make that first call before any stream capture. All calls share the array, which keeps the
+ * make that first call before any stream capture. After cudaDeviceReset the device has a new
+ * context, and the next call resolves the address again (again: not during a capture). All calls share the array, which keeps the
  * last call's contents: calls that overlap on the GPU (different streams, or different host
  * threads on one device) race and give wrong results; order them on one stream. Larger sizes
  * are rejected with ZKG_EINVAL ("log_n must be in 10..=16 for zkg_ntt_noalloc, got N"). */
@@ -327,22 +328,12 @@ int zkg_ntt_pass_times(zkg_ntt *ntt, zkg_stage_time *out, size_t cap, size_t *co
 
 /* ------------------------------------------------------------------ testing and set-up helpers */
 
-/* Throughput probe of the integer multiply-add pipe (the reference's examples/field_bench.rs
- * measures mulmods per second the same way): variant 0 = mad.lo.u32, 1 = mad.hi.u32,
- * 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq Montgomery
- * products, 4 = mul.wide.u32 (32x32 -> 64-bit products), 5 = add.cc / addc.u32 (integer adds),
- * 6 = Fq products in an alternative form (plain mul.wide products, two add chains per row),
- * 7 / 8 = products mixing the two forms (product rows / reduction rows in the production form);
- * 9 = fma.rn.f64 (the double-precision pipe), 10 = the same FMAs interleaved with mul.wide.u32
- * (counts the FMAs only: equal to 9 when the two pipes issue concurrently), 11 = Fq Montgomery
- * products on the double-precision pipe (five 52-bit limbs, R = 2^260), 12 = the same with each
- * column summed as one expression; 13 / 14 = the FMAs of 9 interleaved with mad.lo.u32 / 64-bit adds
- * (FMAs counted); 15 / 16 / 17 = the double-precision product with the product-phase column adds,
- * every column add, or the low halves' adds issued as integer multiply-adds by 1; 18 / 19 = one
- * dependent chain of Fq products on a single thread (integer / double-precision form; products
- * per second = 1 / latency); 20 / 21 / 22 = a chain of XYZZ doublings on one thread with inlined
- * products / one out-of-line product per call / two per call (doublings per second);
- * alternative forms are first checked on the device against the production product.
+/* Peak-rate probes, the denominators of the measured roofline fractions (the reference's
+ * examples/field_bench.rs measures mulmods per second the same way): variant 0 = mad.lo.u32,
+ * 1 = mad.hi.u32, 2 = carry-chained mad.lo.cc / madc.hi.cc (the Montgomery rows' form), 3 = Fq
+ * Montgomery products (integer form), 9 = fma.rn.f64 (the double-precision pipe), 11 = Fq
+ * Montgomery products on the double-precision pipe (five 52-bit limbs, R = 2^260; checked on the
+ * device against the integer form before it is timed). Other variants: ZKG_EINVAL.
  * *ops_per_second receives multiply-adds (or products, or FMAs) per second on the context's
  * device; the best of five launches over every SM. */
 int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);

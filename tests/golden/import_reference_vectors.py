@@ -1,5 +1,7 @@
-"""Copies zk-gpu's golden vectors into this repository (run once, in a checkout that has the
-reference at /root/reference; the GPU machines do not).
+"""Copies zk-gpu's golden vectors into this repository (run once, on a machine with a checkout of
+the reference; the argument is that checkout's tests/golden directory).
+
+    python tests/golden/import_reference_vectors.py <zk-gpu checkout>/tests/golden
 
 The two files are the reference's own fixtures, tests/golden/ntt.json and tests/golden/msm.json,
 generated by the reference's tools/golden/gen.mjs with ffjavascript 0.3.1 (bn128) and licensed
@@ -11,7 +13,6 @@ import pathlib
 import shutil
 import sys
 
-SRC = pathlib.Path("/root/reference/tests/golden")
 DST = pathlib.Path(__file__).resolve().parent
 FILES = ["ntt.json", "msm.json"]
 
@@ -21,6 +22,9 @@ def digest(path: pathlib.Path) -> str:
 
 
 if __name__ == "__main__":
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    SRC = pathlib.Path(sys.argv[1])
     if not SRC.is_dir():
         sys.exit(f"reference vectors not found under {SRC}")
     for name in FILES:

@@ -1,10 +1,10 @@
-"""Batched execution (one CUDA graph, lanes as independent branches) gives exactly the results
-of the same operations run one call at a time."""
+"""Batched execution (one CUDA graph, lanes as independent branches) gives exactly the oracle's
+results, and the same as the operations run one call at a time."""
 import numpy as np
 import pytest
 
-from common import random_fr, random_points
-from oracle import bn254
+from common import msm_ref, random_fr, random_points
+from oracle import bn254, cpu
 from zk_gpu import Batch, CosetShift, Group, Msm, Ntt, ZkGpuError, xyzz_to_affine, xyzz_to_affine_g2
 from zk_gpu.msm import affine_words
 
@@ -24,7 +24,8 @@ def test_uneven_batch_matches_single_calls(gpu):
     expected, outputs = [], []
     for lane, (group, n) in enumerate(rnd_sizes):
         gname = "G1" if group == Group.G1 else "G2"
-        bases = Msm.upload_bases(gpu, random_points(gname, 500 + lane, n))
+        points = random_points(gname, 500 + lane, n)
+        bases = Msm.upload_bases(gpu, points)
         for rep in range(2):  # two MSMs with the same plan in one lane
             s = random_fr(600 + 10 * lane + rep, n)
             sbuf = gpu.buffer(s)
@@ -33,7 +34,9 @@ def test_uneven_batch_matches_single_calls(gpu):
             out = gpu.empty_buffer(group.xyzz_words())
             batch.add_msm(plan, bases, sbuf, out, lane=lane)
             outputs.append((group, out))
-            expected.append(plain_msm(gpu, group, bases, s, n))
+            want = msm_ref(gname, points, s)
+            assert np.array_equal(plain_msm(gpu, group, bases, s, n), want), (gname, n)
+            expected.append(want)
     # an NTT chain (inverse, coset shift, forward) in its own lane, and another transform
     x = random_fr(700, 1 << 15)
     data = gpu.buffer(x)
@@ -47,15 +50,15 @@ def test_uneven_batch_matches_single_calls(gpu):
     data2 = gpu.buffer(y)
     batch.add_ntt(Ntt(gpu, 12), data2, lane=nl + 1)
 
+    want_chain = cpu.ntt(cpu.coset_shift(cpu.ntt(x, inverse=True), np.array(bn254.words32(7), dtype=np.uint32)))
+    want2 = cpu.ntt(y)
+    # the same chain one call at a time
     ref = gpu.buffer(x)
     ntt_ref = Ntt(gpu, 15)
     ntt_ref.inverse(gpu, ref)
     CosetShift(gpu, 15, 7).shift(gpu, ref)
     ntt_ref.forward(gpu, ref)
-    want_chain = gpu.read(ref, x.size)
-    ref2 = gpu.buffer(y)
-    Ntt(gpu, 12).forward(gpu, ref2)
-    want2 = gpu.read(ref2, y.size)
+    assert np.array_equal(gpu.read(ref, x.size), want_chain)
 
     batch.launch()
     gpu.wait()

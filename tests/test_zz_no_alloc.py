@@ -31,7 +31,11 @@ def plan_result(gpu, x, log_n, inverse):
 def test_matches_the_plan_entry_points_call_after_call(gpu):
     # Two calls in a row on the largest size, then a smaller size and back: the shared scratch
     # keeps each call's contents, which must never leak into the next result.
-    for log_n, inverse, seed in [(16, False, 1), (16, True, 2), (12, True, 3), (16, False, 4)]:
+    # log_n 10 and 11 take the one-pass branch (the tile is the whole transform and the scratch
+    # array holds only the twiddles).
+    cases = [(16, False, 1), (16, True, 2), (12, True, 3), (16, False, 4), (10, False, 6), (10, True, 7),
+             (11, False, 8), (11, True, 9), (16, True, 10)]
+    for log_n, inverse, seed in cases:
         x = random_fr(seed, 1 << log_n)
         buf = gpu.buffer(x)
         noalloc(gpu, buf, log_n, inverse)
@@ -39,11 +43,12 @@ def test_matches_the_plan_entry_points_call_after_call(gpu):
         assert np.array_equal(got, plan_result(gpu, x, log_n, inverse)), (log_n, inverse)
 
 
-def test_round_trip(gpu):
-    x = random_fr(5, 1 << 14)
+@pytest.mark.parametrize("log_n", [10, 11, 14])
+def test_round_trip(gpu, log_n):
+    x = random_fr(5 + log_n, 1 << log_n)
     buf = gpu.buffer(x)
-    noalloc(gpu, buf, 14, False)
-    noalloc(gpu, buf, 14, True)
+    noalloc(gpu, buf, log_n, False)
+    noalloc(gpu, buf, log_n, True)
     assert np.array_equal(gpu.read(buf, x.size), x)
 
 

@@ -545,7 +545,6 @@ int zkg_bench_integer_pipe(zkg_ctx* ctx, int variant, double* ops_per_second) {
   return guard([&] {
     need(ctx, "ctx");
     need(ops_per_second, "ops_per_second");
-    if (variant < 0 || variant > 22) fail(ZKG_EINVAL, "variant must be 0..22");
     *ops_per_second = bench_integer_pipe(ctx, variant);
   });
 }

@@ -259,10 +259,9 @@ __device__ __forceinline__ Fp<P> mont_mul_inline(const Fp<P>& a, const Fp<P>& b)
   return r;
 }
 
-// Alternative product for comparison (zkg_bench_integer_pipe variant 6): plain mul.wide products
-// (no 64-bit addend to assemble) and two add chains per row, one for the low halves and one
-// for the high halves one word up; more work on the integer add pipe, less on the multiply
-// pipe. t[i+8] is fresh in a product row and accumulates in a reduction row.
+// Add chains for rows of plain mul.wide products (no 64-bit addend to assemble): one chain for
+// the low halves and one for the high halves one word up. t[i+8] is fresh in a product row and
+// accumulates in a reduction row.
 #define ZKG_ADD_LO_FRESH(t, i, d)                                                                \
   asm("add.cc.u32  %0, %0, %9;\n\t"                                                              \
       "addc.cc.u32 %1, %1, %10;\n\t"                                                             \
@@ -306,51 +305,8 @@ __device__ __forceinline__ Fp<P> mont_mul_inline(const Fp<P>& a, const Fp<P>& b)
         "r"((uint32_t)(d[3] >> 32)), "r"((uint32_t)(d[4] >> 32)), "r"((uint32_t)(d[5] >> 32)),    \
         "r"((uint32_t)(d[6] >> 32)), "r"((uint32_t)(d[7] >> 32)))
 
-template <class P>
-__device__ __forceinline__ Fp<P> mont_mul_v2(const Fp<P>& a, const Fp<P>& b) {
-  constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};
-  uint32_t t[17];
-#pragma unroll
-  for (int i = 0; i < 8; i++) t[i] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    uint64_t d[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = (uint64_t)a.w[j] * b.w[i];
-    ZKG_ADD_LO_FRESH(t, i, d);
-    ZKG_ADD_HI(t, i, d);
-    const uint32_t m = t[i] * P::INV;
-#pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = (uint64_t)m * q[j];
-    ZKG_ADD_LO_ACC(t, i, d);
-    ZKG_ADD_HI(t, i, d);
-  }
-  Fp<P> s, d;
-#pragma unroll
-  for (int i = 0; i < 8; i++) s.w[i] = t[8 + i];
-  uint32_t borrow;
-  asm("sub.cc.u32  %0, %9, %17;\n\t"
-      "subc.cc.u32 %1, %10, %18;\n\t"
-      "subc.cc.u32 %2, %11, %19;\n\t"
-      "subc.cc.u32 %3, %12, %20;\n\t"
-      "subc.cc.u32 %4, %13, %21;\n\t"
-      "subc.cc.u32 %5, %14, %22;\n\t"
-      "subc.cc.u32 %6, %15, %23;\n\t"
-      "subc.cc.u32 %7, %16, %24;\n\t"
-      "subc.u32    %8, 0, 0;"
-      : "=&r"(d.w[0]), "=&r"(d.w[1]), "=&r"(d.w[2]), "=&r"(d.w[3]), "=&r"(d.w[4]), "=&r"(d.w[5]), "=&r"(d.w[6]),
-        "=&r"(d.w[7]), "=&r"(borrow)
-      : "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7]),
-        "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
-  Fp<P> r;
-#pragma unroll
-  for (int i = 0; i < 8; i++) r.w[i] = (s.w[i] & borrow) | (d.w[i] & ~borrow);
-  return r;
-}
-
-// Mixed forms for comparison (zkg_bench_integer_pipe variants 7 and 8): one row kind with
-// mad.wide + one chain, the other with mul.wide + two chains. PROD_WIDE selects the product rows'
-// form (true: mad.wide), the reduction rows take the other.
+// Mixed forms: one row kind with mad.wide + one chain, the other with mul.wide + two chains.
+// PROD_WIDE selects the product rows' form (true: mad.wide), the reduction rows take the other.
 template <class P, bool PROD_WIDE>
 __device__ __forceinline__ Fp<P> mont_mul_mixed(const Fp<P>& a, const Fp<P>& b) {
   constexpr uint32_t q[8] = {P::P0, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};

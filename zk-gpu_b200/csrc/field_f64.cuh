@@ -119,140 +119,6 @@ __device__ __forceinline__ void mont_mul(const double (&x)[5], const double (&y)
   }
 }
 
-// acc += x as two integer multiply-adds by `one` (which must be 1 and unknown to the compiler):
-// the add then issues on the integer multiply-add pipe instead of the integer ALU.
-__device__ __forceinline__ void add64_mad(uint64_t& acc, uint64_t x, uint32_t one) {
-  uint32_t lo = (uint32_t)acc, hi = (uint32_t)(acc >> 32);
-  asm("mad.lo.cc.u32 %0, %2, %4, %0;\n\tmadc.lo.u32 %1, %3, %4, %1;"
-      : "+r"(lo), "+r"(hi)
-      : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)), "r"(one));
-  acc = lo | (uint64_t)hi << 32;
-}
-
-// mont_mul with a share of the column adds moved to the multiply-add pipe: MODE 1 = the
-// product-phase adds, 2 = every column add, 3 = the low halves' adds only.
-template <typename L, int MODE>
-__device__ __forceinline__ void mont_mul_split(const double (&x)[5], const double (&y)[5], double (&out)[5],
-                                               uint32_t one) {
-  uint64_t c[10];
-#pragma unroll
-  for (int k = 0; k < 10; k++) c[k] = 0ull - column_bias(k);
-#pragma unroll
-  for (int i = 0; i < 5; i++) {
-#pragma unroll
-    for (int j = 0; j < 5; j++) {
-      double h = __fma_rz(x[i], y[j], kC104);
-      double l = __fma_rn(x[i], y[j], __dsub_rn(kC104p52, h));
-      if (MODE == 1 || MODE == 2 || MODE == 3)
-        add64_mad(c[i + j], bits(l), one);
-      else
-        c[i + j] += bits(l);
-      if (MODE == 1 || MODE == 2)
-        add64_mad(c[i + j + 1], bits(h), one);
-      else
-        c[i + j + 1] += bits(h);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 5; i++) {
-    const uint64_t t = c[i];
-    const uint64_t tl = t & kM52;
-    const uint64_t carry = (t >> 52) + (tl != 0 ? 1ull : 0ull);
-    const double tf = limb_to_double(tl);
-    const double qh = __fma_rz(tf, (double)L::PINV, kC104);
-    const double ql = __fma_rn(tf, (double)L::PINV, __dsub_rn(kC104p52, qh));
-    const double q = __dsub_rn(ql, kC52);
-    c[i + 1] += bits(__fma_rz(q, (double)L::P(0), kC104)) + carry;
-#pragma unroll
-    for (int j = 1; j < 5; j++) {
-      double h = __fma_rz(q, (double)L::P(j), kC104);
-      double l = __fma_rn(q, (double)L::P(j), __dsub_rn(kC104p52, h));
-      if (MODE == 2 || MODE == 3)
-        add64_mad(c[i + j], bits(l), one);
-      else
-        c[i + j] += bits(l);
-      if (MODE == 2)
-        add64_mad(c[i + j + 1], bits(h), one);
-      else
-        c[i + j + 1] += bits(h);
-    }
-  }
-  uint64_t carry = 0;
-#pragma unroll
-  for (int k = 5; k < 10; k++) {
-    const uint64_t v = c[k] + carry;
-    carry = v >> 52;
-    out[k - 5] = limb_to_double(k < 9 ? (v & kM52) : v);
-  }
-}
-
-// The same product with every column formed as one sum over all its terms (the split halves are
-// produced first), which lets the compiler use three-input adds.
-template <typename L>
-__device__ __forceinline__ void mont_mul_tree(const double (&x)[5], const double (&y)[5], double (&out)[5]) {
-  uint64_t lo[5][5], hi[5][5];
-#pragma unroll
-  for (int i = 0; i < 5; i++) {
-#pragma unroll
-    for (int j = 0; j < 5; j++) {
-      double h = __fma_rz(x[i], y[j], kC104);
-      double l = __fma_rn(x[i], y[j], __dsub_rn(kC104p52, h));
-      lo[i][j] = bits(l);
-      hi[i][j] = bits(h);
-    }
-  }
-  uint64_t c[10];
-#pragma unroll
-  for (int k = 0; k < 10; k++) {
-    uint64_t s = 0ull - column_bias(k);
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-      const int j = k - i, jh = k - 1 - i;
-      if (j >= 0 && j < 5) s += lo[i][j];
-      if (jh >= 0 && jh < 5) s += hi[i][jh];
-    }
-    c[k] = s;
-  }
-  uint64_t rlo[5][5], rhi[5][5];
-#pragma unroll
-  for (int i = 0; i < 5; i++) {
-    uint64_t t = c[i];
-#pragma unroll
-    for (int i2 = 0; i2 < i; i2++) {  // reduction terms of earlier digits that land in column i
-      const int j = i - i2, jh = i - 1 - i2;
-      if (j >= 1 && j < 5) t += rlo[i2][j];
-      if (jh >= 0 && jh < 5) t += rhi[i2][jh];
-    }
-    const uint64_t tl = t & kM52;
-    const uint64_t carry = (t >> 52) + (tl != 0 ? 1ull : 0ull);
-    const double tf = limb_to_double(tl);
-    const double qh = __fma_rz(tf, (double)L::PINV, kC104);
-    const double ql = __fma_rn(tf, (double)L::PINV, __dsub_rn(kC104p52, qh));
-    const double q = __dsub_rn(ql, kC52);
-    rhi[i][0] = bits(__fma_rz(q, (double)L::P(0), kC104)) + carry;
-#pragma unroll
-    for (int j = 1; j < 5; j++) {
-      double h = __fma_rz(q, (double)L::P(j), kC104);
-      double l = __fma_rn(q, (double)L::P(j), __dsub_rn(kC104p52, h));
-      rlo[i][j] = bits(l);
-      rhi[i][j] = bits(h);
-    }
-  }
-  uint64_t carry = 0;
-#pragma unroll
-  for (int k = 5; k < 10; k++) {
-    uint64_t v = c[k] + carry;
-#pragma unroll
-    for (int i2 = 0; i2 < 5; i2++) {
-      const int j = k - i2, jh = k - 1 - i2;
-      if (j >= 1 && j < 5) v += rlo[i2][j];
-      if (jh >= 0 && jh < 5) v += rhi[i2][jh];
-    }
-    carry = v >> 52;
-    out[k - 5] = limb_to_double(k < 9 ? (v & kM52) : v);
-  }
-}
-
 // Bias of the reduction phase's patterns in column k (the product phase of mont_mul_sub adds
 // and subtracts equal numbers of patterns, whose biases cancel).
 constexpr int red_lo_terms(int k) {

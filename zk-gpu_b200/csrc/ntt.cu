@@ -551,21 +551,48 @@ __global__ void ntt_twiddles_pow(Fr w, uint32_t count, uint32_t* __restrict__ ou
   store_fe(out + 8 * (size_t)j, acc);
 }
 
-// Device address of g_noalloc_scratch per device, resolved once with that device current (in
-// host code the symbol names a host-side stand-in, not device memory).
+// Device address of g_noalloc_scratch per device, resolved with that device current (in host
+// code the symbol names a host-side stand-in, not device memory). The cache is keyed on the
+// device's current context as well: after cudaDeviceReset the device gets a new context, the
+// old address is stale, and the next call resolves it again (and sets the kernels'
+// shared-memory limit again, a per-context attribute).
 static std::mutex g_noalloc_mutex;
-static uint32_t* g_noalloc_ptr[64];
+struct NoAllocScratch {
+  void* context;
+  uint32_t* ptr;
+};
+static NoAllocScratch g_noalloc_cache[64];
+
+using CtxGetCurrentFn = int (*)(void**);
+static CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  if (!fn) fail(ZKG_ECUDA, "cuCtxGetCurrent is not available from the CUDA driver");
+  return fn;
+}
 
 static uint32_t* noalloc_scratch(int device) {
   if (device < 0 || device >= 64) fail(ZKG_ENODEV, "device index out of range");
+  void* context = nullptr;  // null before the runtime has made the device's context
+  if (ctx_get_current()(&context) != 0) fail(ZKG_ECUDA, "cuCtxGetCurrent failed");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[device]) {
+  NoAllocScratch& e = g_noalloc_cache[device];
+  if (!e.ptr || !context || e.context != context) {
     void* p = nullptr;
+    // The first runtime call that needs the device also makes its context current.
     check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
+    if (ctx_get_current()(&context) != 0 || !context) fail(ZKG_ECUDA, "no current CUDA context");
     set_pass_smem_limits();
-    g_noalloc_ptr[device] = static_cast<uint32_t*>(p);
+    e.context = context;
+    e.ptr = static_cast<uint32_t*>(p);
   }
-  return g_noalloc_ptr[device];
+  return e.ptr;
 }
 
 static void ntt_noalloc(uint32_t log_n, int inverse, uint32_t* data, cudaStream_t s) {

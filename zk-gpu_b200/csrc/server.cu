@@ -34,6 +34,20 @@ static double now_ms() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Text of the exception being handled (inside a catch block): a failed request records it
+// instead of letting the exception leave a server thread, which would end the process.
+static std::string current_error_text() {
+  try {
+    throw;
+  } catch (const Error& e) {
+    return e.msg;
+  } catch (const std::exception& e) {
+    return std::string("internal error: ") + e.what();
+  } catch (...) {
+    return "unexpected internal error";
+  }
+}
+
 ServerSlot::~ServerSlot() {
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
@@ -84,7 +98,10 @@ int Server::add_key(size_t n, const zkg_buf* g1, const zkg_buf* g2) {
   return (int)keys.size() - 1;
 }
 
+// Takes mu: add_key may grow the key list from another thread at the same time. The keys
+// themselves live behind unique_ptr, so the pointer returned stays valid after the lock ends.
 const ServerKey* Server::key_for(uint32_t log_m) const {
+  std::lock_guard<std::mutex> lock(mu);
   const ServerKey* best = nullptr;
   const size_t m = (size_t)1 << log_m;
   for (auto& k : keys)
@@ -315,12 +332,13 @@ void Server::dispatcher() {
     for (auto& rs : ready) {
       try {
         launch(rs.first, rs.second);
-      } catch (const Error& e) {
+      } catch (...) {
+        const std::string msg = current_error_text();
         std::lock_guard<std::mutex> lock(mu);
         rs.second->busy = false;
         rs.second->req = nullptr;
         rs.first->state = 3;
-        rs.first->error = e.msg;
+        rs.first->error = msg;
         rs.first->t_done = now_ms();
         cv.notify_all();
       }
@@ -359,7 +377,8 @@ void Server::builder() {
         slots.push_back(std::move(s));
       }
       launch(r, slot);
-    } catch (const Error& e) {
+    } catch (...) {
+      const std::string msg = current_error_text();
       std::lock_guard<std::mutex> lock(mu);
       if (!slot) {
         bytes_used -= std::min(bytes_used, job.second);
@@ -369,7 +388,7 @@ void Server::builder() {
         slot->req = nullptr;
       }
       r->state = 3;
-      r->error = e.msg;
+      r->error = msg;
       r->t_done = now_ms();
     }
     cv.notify_all();

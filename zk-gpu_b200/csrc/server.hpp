@@ -70,7 +70,7 @@ struct Server {
   uint64_t slots_created = 0, slots_evicted = 0, completed = 0;
   double build_ms = 0;
   bool stopping = false;
-  std::mutex mu;
+  mutable std::mutex mu;
   std::condition_variable cv;  // queue, slot, build and completion changes
   std::thread dispatcher_thread, builder_thread;
 

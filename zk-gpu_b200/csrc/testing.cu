@@ -164,11 +164,16 @@ void generator_multiples(zkg_ctx* ctx, int group, const zkg_buf* scalars, size_t
   check_cuda(cudaStreamSynchronize(ctx->stream), "generator multiples");
 }
 
-// ------------------------------------------------------------------ integer pipe throughput
+// ------------------------------------------------------------------ roofline denominators
+//
+// Peak rates measured on the running GPU, the denominators of the bench line's fractions:
+// variant 0: mad.lo.u32, 1: mad.hi.u32, 2: a carry chain of mad.lo.cc / madc.hi.cc as in the
+// Montgomery rows (8 multiply-adds per step each), 3: Fq Montgomery products in the library's
+// integer form, 9: fma.rn.f64, 11: Fq products in the double-precision limb form (checked
+// equal to the integer form on the device before it is timed).
 
 // Eight independent multiply-add chains per thread (enough independent work to keep the pipe
-// full at any occupancy). variant 0: mad.lo.u32, 1: mad.hi.u32, 2: a carry chain of
-// mad.lo.cc / madc.hi.cc as in the Montgomery rows. Each inner step is 8 multiply-adds.
+// full at any occupancy).
 template <int V>
 __global__ void imad_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
   uint32_t a[8];
@@ -180,20 +185,6 @@ __global__ void imad_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
     for (int j = 0; j < 8; j++) {
       if (V == 0) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(b), "r"(a[(j + 1) & 7]));
       if (V == 1) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(b), "r"(a[(j + 1) & 7]));
-    }
-    if (V == 4) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2) {
-        uint64_t p;
-        asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(p) : "r"(a[j]), "r"(b));
-        a[j] = (uint32_t)p ^ a[j + 1];
-        a[j + 1] = (uint32_t)(p >> 32);
-      }
-    }
-    if (V == 5) {
-#pragma unroll
-      for (int j = 0; j < 8; j++)
-        asm volatile("add.cc.u32 %0, %0, %1;\n\taddc.u32 %1, %1, %2;" : "+r"(a[j]), "+r"(a[(j + 3) & 7]) : "r"(b));
     }
     if (V == 2)
       asm volatile(
@@ -214,55 +205,20 @@ __global__ void imad_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
   if (x == 0x9e3779b9u) out[0] = x;  // keeps the chains live
 }
 
-// FP64 pipe throughput: eight independent fma.rn.f64 chains (variant 9), and the same chains
-// interleaved with four mul.wide.u32 per step (variant 10), eight mad.lo.u32 (13) or four 64-bit
-// integer adds (14), to see which pipes issue concurrently with the double-precision one. Values
-// stay normal (b < 1, c > 0).
-template <int V>
+// FP64 pipe throughput: eight independent fma.rn.f64 chains. Values stay normal (b < 1, c > 0).
 __global__ void dfma_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
   double d[8];
-  uint32_t a[8];
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    d[j] = 1.0 + 1e-3 * (double)((threadIdx.x + 31u * j) & 1023u);
-    a[j] = (threadIdx.x + 977u * j) ^ seed;
-  }
+  for (int j = 0; j < 8; j++) d[j] = 1.0 + 1e-3 * (double)((threadIdx.x + 31u * j + seed) & 1023u);
   const double b = 0.9999999, c = 1e-3;
-  const uint32_t m = seed | 1u;
   for (uint32_t it = 0; it < iters; it++) {
 #pragma unroll
     for (int j = 0; j < 8; j++) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(d[j]) : "d"(b), "d"(c));
-    if (V == 13) {
-#pragma unroll
-      for (int j = 0; j < 8; j++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(m), "r"(a[(j + 1) & 7]));
-    }
-    if (V == 14) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2) {
-        uint64_t u = (uint64_t)a[j] | (uint64_t)a[j + 1] << 32;
-        asm volatile("add.u64 %0, %0, %1;" : "+l"(u) : "l"((uint64_t)m * 0x100000001ull));
-        a[j] = (uint32_t)u;
-        a[j + 1] = (uint32_t)(u >> 32);
-      }
-    }
-    if (V == 10) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2) {
-        uint64_t p;
-        asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(p) : "r"(a[j]), "r"(m));
-        a[j] = (uint32_t)p ^ a[j + 1];
-        a[j + 1] = (uint32_t)(p >> 32);
-      }
-    }
   }
   double s = 0;
-  uint32_t x = 0;
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    s += d[j];
-    x ^= a[j];
-  }
-  if (s == 12345.0 || x == 0x9e3779b9u) out[0] = x;  // keeps the chains live
+  for (int j = 0; j < 8; j++) s += d[j];
+  if (s == 12345.0) out[0] = 1;  // keeps the chains live
 }
 
 // Fq Montgomery products per second (the reference's examples/field_bench.rs idea).
@@ -276,50 +232,6 @@ __global__ void mulmod_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
     z = z * y;
   }
   if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
-}
-
-// The alternative product (mont_mul_v2), same loop as mulmod_kernel.
-__global__ void mulmod_v2_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
-  Fq x = Fq::one(), y = Fq::one();
-  x.w[0] ^= threadIdx.x + seed;
-  y.w[1] ^= blockIdx.x;
-  Fq z = x;
-  for (uint32_t it = 0; it < iters; it++) {
-    x = mont_mul_v2(x, y);
-    z = mont_mul_v2(z, y);
-  }
-  if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
-}
-
-template <bool PROD_WIDE>
-__global__ void mulmod_mixed_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
-  Fq x = Fq::one(), y = Fq::one();
-  x.w[0] ^= threadIdx.x + seed;
-  y.w[1] ^= blockIdx.x;
-  Fq z = x;
-  for (uint32_t it = 0; it < iters; it++) {
-    x = mont_mul_mixed<FqParams, PROD_WIDE>(x, y);
-    z = mont_mul_mixed<FqParams, PROD_WIDE>(z, y);
-  }
-  if ((x.w[0] ^ z.w[3]) == 0x9e3779b9u) out[0] = x.w[0];
-}
-
-// Counts threads whose alternative-form chain differs from the operator* chain (0 expected).
-template <int FORM>
-__global__ void mulmod_compare_kernel(uint32_t* mismatches, uint32_t iters) {
-  Fq x = Fq::one(), y = Fq::one();
-  x.w[0] ^= threadIdx.x * 2654435761u + blockIdx.x;
-  x.w[7] &= 0x0fffffffu;
-  y.w[2] ^= blockIdx.x * 40503u + 7u;
-  y.w[7] &= 0x0fffffffu;
-  Fq u = x, v = x;
-  for (uint32_t it = 0; it < iters; it++) {
-    u = u * y;
-    if (FORM == 6) v = mont_mul_v2(v, y);
-    if (FORM == 7) v = mont_mul_mixed<FqParams, true>(v, y);
-    if (FORM == 8) v = mont_mul_mixed<FqParams, false>(v, y);
-  }
-  if (u != v) atomicAdd(mismatches, 1u);
 }
 
 // Fq products on the double-precision pipe (field_f64.cuh), same loop as mulmod_kernel.
@@ -339,72 +251,6 @@ __global__ void mulmod_f64_kernel(uint32_t* out, uint32_t iters, uint32_t seed) 
   if (x[0] == z[3] + 0.5) out[0] = (uint32_t)x[1];  // keeps the chains live
 }
 
-__global__ void mulmod_f64_tree_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
-  double x[5], y[5], z[5];
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-    const uint64_t m = k < 4 ? f64::kM52 : 0xffffffffull;
-    x[k] = f64::limb_to_double(((uint64_t)(threadIdx.x + seed) * 0x9e3779b97f4a7c15ull >> (7 * k)) & m);
-    y[k] = f64::limb_to_double(((uint64_t)(blockIdx.x + 977u * k) * 0xd1b54a32d192ed03ull) & m);
-    z[k] = y[k];
-  }
-  for (uint32_t it = 0; it < iters; it++) {
-    f64::mont_mul_tree<f64::FqLimbs>(x, y, x);
-    f64::mont_mul_tree<f64::FqLimbs>(z, y, z);
-  }
-  if (x[0] == z[3] + 0.5) out[0] = (uint32_t)x[1];  // keeps the chains live
-}
-
-template <int MODE>
-__global__ void mulmod_f64_split_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
-  const uint32_t one = seed / 12345u;  // 1, not known to the compiler
-  double x[5], y[5], z[5];
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-    const uint64_t m = k < 4 ? f64::kM52 : 0xffffffffull;
-    x[k] = f64::limb_to_double(((uint64_t)(threadIdx.x + seed) * 0x9e3779b97f4a7c15ull >> (7 * k)) & m);
-    y[k] = f64::limb_to_double(((uint64_t)(blockIdx.x + 977u * k) * 0xd1b54a32d192ed03ull) & m);
-    z[k] = y[k];
-  }
-  for (uint32_t it = 0; it < iters; it++) {
-    f64::mont_mul_split<f64::FqLimbs, MODE>(x, y, x, one);
-    f64::mont_mul_split<f64::FqLimbs, MODE>(z, y, z, one);
-  }
-  if (x[0] == z[3] + 0.5) out[0] = (uint32_t)x[1];  // keeps the chains live
-}
-
-// One dependent chain of products on a single thread: the latency of one product (variants 18:
-// integer, 19: double-precision limbs; out-of-line forms, as the single-thread kernels use).
-__global__ void mulmod_latency_kernel(uint32_t* out, uint32_t iters, uint32_t seed, int f64_form) {
-  if (f64_form) {
-    f64::FqD x, y;
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-      x.l[k] = f64::limb_to_double(((uint64_t)(seed + 3u * k) * 0x9e3779b97f4a7c15ull) & (k < 4 ? f64::kM52 : 0xffffull));
-      y.l[k] = f64::limb_to_double(((uint64_t)(seed + 7u * k) * 0xd1b54a32d192ed03ull) & (k < 4 ? f64::kM52 : 0xffffull));
-    }
-    for (uint32_t it = 0; it < iters; it++) x = f64::fqd_mul_call(x, y);
-    if (x.l[0] == 0.5) out[0] = 1;
-  } else {
-    FqC x = FqC::one(), y = FqC::one();
-    x.w[0] ^= seed;
-    y.w[1] ^= seed * 3u;
-    for (uint32_t it = 0; it < iters; it++) x = x * y;
-    if (x.w[0] == 0x9e3779b9u) out[0] = x.w[1];
-  }
-}
-
-// A chain of XYZZ doublings on one thread (the combine stage's critical path), in a given
-// product form: variants 20 (inlined), 21 (one out-of-line product per call), 22 (pairs).
-template <class F>
-__global__ void doubling_chain_kernel(uint32_t* out, uint32_t iters, uint32_t seed) {
-  Xyzz<F> p{F::one(), F::one(), F::one(), F::one()};
-  p.x.w[0] ^= seed;
-  p.y.w[1] ^= seed * 7u;
-  for (uint32_t it = 0; it < iters; it++) p = xyzz_double(p);
-  if (p.x.w[0] == 0x9e3779b9u) out[0] = p.y.w[0];
-}
-
 // 16 a mod p for a canonical Fq value: the factor between Montgomery forms with R = 2^256 and
 // R = 2^260 of the same element.
 __device__ __forceinline__ Fq times16(Fq a) {
@@ -414,9 +260,7 @@ __device__ __forceinline__ Fq times16(Fq a) {
 }
 
 // Counts threads whose double-precision product chain differs from the integer chain.
-template <int FORM>
-__global__ void mulmod_f64_compare_kernel(uint32_t* mismatches, uint32_t iters, uint32_t seed) {
-  const uint32_t one = seed / 12345u;
+__global__ void mulmod_f64_compare_kernel(uint32_t* mismatches, uint32_t iters) {
   Fq x = Fq::one(), y = Fq::one();
   x.w[0] ^= threadIdx.x * 2654435761u + blockIdx.x;
   x.w[7] &= 0x0fffffffu;
@@ -430,9 +274,7 @@ __global__ void mulmod_f64_compare_kernel(uint32_t* mismatches, uint32_t iters, 
   Fq u = x;
   for (uint32_t it = 0; it < iters; it++) {
     u = u * y;
-    if (FORM == 0) f64::mont_mul<f64::FqLimbs>(a, b, a);
-    if (FORM == 1) f64::mont_mul_tree<f64::FqLimbs>(a, b, a);
-    if (FORM >= 2) f64::mont_mul_split<f64::FqLimbs, FORM - 1>(a, b, a, one);
+    f64::mont_mul<f64::FqLimbs>(a, b, a);
   }
   uint32_t w[8];
   f64::limbs_to_words(a, w);
@@ -452,68 +294,26 @@ __global__ void mulmod_f64_compare_kernel(uint32_t* mismatches, uint32_t iters, 
   if (!same && !same_p) atomicAdd(mismatches, 1u);
 }
 
+bool integer_pipe_variant_known(int variant) {
+  return variant == 0 || variant == 1 || variant == 2 || variant == 3 || variant == 9 || variant == 11;
+}
+
 double bench_integer_pipe(zkg_ctx* ctx, int variant) {
+  if (!integer_pipe_variant_known(variant)) fail(ZKG_EINVAL, "variant must be one of 0, 1, 2, 3, 9, 11");
   use(ctx);
   DeviceArray sink;
   sink.alloc(16, "sink");
   const unsigned blocks = (unsigned)ctx->sm_count * 8, threads = 256;
-  const bool product = variant == 3 || (variant >= 6 && variant <= 8) || variant == 11 || variant == 12 || variant >= 15;
-  if (variant >= 20 && variant <= 22) {  // doublings per second on one thread
-    const uint32_t chain = 2048;
-    cudaEvent_t e0, e1;
-    check_cuda(cudaEventCreate(&e0), "event");
-    check_cuda(cudaEventCreate(&e1), "event");
-    auto go = [&](uint32_t iters) {
-      if (variant == 20) doubling_chain_kernel<Fq><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
-      if (variant == 21) doubling_chain_kernel<FqC><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
-      if (variant == 22) doubling_chain_kernel<FqCP><<<1, 1, 0, ctx->stream>>>(sink.ptr, iters, 12345u);
-      check_launch("doubling_chain_kernel");
-    };
-    go(16);
-    check_cuda(cudaEventRecord(e0, ctx->stream), "event");
-    go(chain);
-    check_cuda(cudaEventRecord(e1, ctx->stream), "event");
-    check_cuda(cudaEventSynchronize(e1), "doubling probe");
-    float ms = 0;
-    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event");
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return chain / (ms * 1e-3);
-  }
-  if (variant == 18 || variant == 19) {  // single-thread latency: products per second of one chain
-    const uint32_t chain = 20000;
-    cudaEvent_t e0, e1;
-    check_cuda(cudaEventCreate(&e0), "event");
-    check_cuda(cudaEventCreate(&e1), "event");
-    mulmod_latency_kernel<<<1, 1, 0, ctx->stream>>>(sink.ptr, 64, 12345u, variant == 19);
-    check_launch("mulmod_latency_kernel");
-    check_cuda(cudaEventRecord(e0, ctx->stream), "event");
-    mulmod_latency_kernel<<<1, 1, 0, ctx->stream>>>(sink.ptr, chain, 12345u, variant == 19);
-    check_launch("mulmod_latency_kernel");
-    check_cuda(cudaEventRecord(e1, ctx->stream), "event");
-    check_cuda(cudaEventSynchronize(e1), "latency probe");
-    float ms = 0;
-    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event");
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return chain / (ms * 1e-3);
-  }
+  const bool product = variant == 3 || variant == 11;
   const uint32_t iters = product ? 256 : 4096;
-  if ((variant >= 6 && variant <= 8) || variant == 11 || variant == 12 || variant >= 15) {  // alternative forms must agree with the production product first
+  if (variant == 11) {  // the limb form must agree with the integer product first
     check_cuda(cudaMemsetAsync(sink.ptr, 0, 4, ctx->stream), "clear");
-    if (variant == 6) mulmod_compare_kernel<6><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
-    if (variant == 7) mulmod_compare_kernel<7><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
-    if (variant == 8) mulmod_compare_kernel<8><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
-    if (variant == 11) mulmod_f64_compare_kernel<0><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64, 12345u);
-    if (variant == 12) mulmod_f64_compare_kernel<1><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64, 12345u);
-    if (variant == 15) mulmod_f64_compare_kernel<2><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64, 12345u);
-    if (variant == 16) mulmod_f64_compare_kernel<3><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64, 12345u);
-    if (variant == 17) mulmod_f64_compare_kernel<4><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64, 12345u);
-    check_launch("mulmod_compare_kernel");
+    mulmod_f64_compare_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, 64);
+    check_launch("mulmod_f64_compare_kernel");
     uint32_t bad = 0;
     check_cuda(cudaMemcpyAsync(&bad, sink.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     check_cuda(cudaStreamSynchronize(ctx->stream), "compare");
-    if (bad) fail(ZKG_ECUDA, "an alternative product form differs from the production one in " + std::to_string(bad) + " threads");
+    if (bad) fail(ZKG_ECUDA, "the double-precision product differs from the integer one in " + std::to_string(bad) + " threads");
   }
   cudaEvent_t a, b;
   check_cuda(cudaEventCreate(&a), "event");
@@ -523,20 +323,8 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
       case 0: imad_kernel<0><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 1: imad_kernel<1><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 2: imad_kernel<2><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 4: imad_kernel<4><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 5: imad_kernel<5><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 6: mulmod_v2_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 7: mulmod_mixed_kernel<true><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 8: mulmod_mixed_kernel<false><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 9: dfma_kernel<9><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 10: dfma_kernel<10><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
+      case 9: dfma_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       case 11: mulmod_f64_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 13: dfma_kernel<13><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 14: dfma_kernel<14><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 15: mulmod_f64_split_kernel<1><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 16: mulmod_f64_split_kernel<2><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 17: mulmod_f64_split_kernel<3><<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
-      case 12: mulmod_f64_tree_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
       default: mulmod_kernel<<<blocks, threads, 0, ctx->stream>>>(sink.ptr, iters, 12345u); break;
     }
     check_launch("integer pipe benchmark");
@@ -555,10 +343,8 @@ double bench_integer_pipe(zkg_ctx* ctx, int variant) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   double threads_total = (double)blocks * threads;
-  // variants 0-2: 8 multiply-adds per step; 3: 2 Fq products per step; 4: 4 wide products per
-  // step; 5: 16 carry adds per step; 9, 10: 8 double-precision FMAs per step (10 also runs 4
-  // wide integer products per step, not counted).
-  double per = product ? 2.0 : variant == 4 ? 4.0 : variant == 5 ? 16.0 : 8.0;
+  // variants 0-2 and 9: 8 multiply-adds (or FMAs) per step; 3 and 11: 2 Fq products per step.
+  double per = product ? 2.0 : 8.0;
   double ops = threads_total * iters * per;
   return ops / (best * 1e-3);
 }
