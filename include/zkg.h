@@ -131,6 +131,11 @@ int zkg_msm_set_variant(zkg_msm *msm, int variant);
  * 1 = the group of the first lane only, 2 = none, 3 = the group of the first pair of
  * neighbouring lanes with equal slots (default). The scatter pass always merges every group. */
 int zkg_msm_set_sort(zkg_msm *msm, int mode);
+/* Counting-sort form (no reference counterpart): 0 = one pass scatters every (window, point)
+ * entry through an atomic cursor per slot; 1 = the counting pass also records each entry's
+ * rank within its slot, and the placing pass writes the entries window by window, so the
+ * stores of one window meet in L2 (default; applies for c <= 16, larger c use 0). */
+int zkg_msm_set_sort_form(zkg_msm *msm, int form);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,
@@ -180,6 +185,49 @@ int zkg_coset_shift(zkg_coset *coset, zkg_buf *data);
  * (its 1/n factor folded into the shift's table): the same words as the two calls, one pass
  * over the data fewer. The coset must cover 2^log_n elements of the transform. */
 int zkg_ntt_inverse_coset(zkg_ntt *ntt, zkg_buf *data, zkg_coset *coset);
+
+/* The pointwise step of a Groth16 witness map on the coset g*H, H the 2^log_n-th roots of unity
+ * (the reference leaves it to callers: "coset shifts and pointwise products, which are simple
+ * kernels on top", README.md:229-230; no reference function): with a, b, c the evaluations of
+ * the three constraint polynomials on g*H, h_i = (a_i b_i - c_i) / (g^N - 1), N = 2^log_n (the
+ * vanishing polynomial x^N - 1 takes the value g^N - 1 everywhere on the coset). All plain Fr
+ * words, natural order; g < r given as 8 plain words, g^N != 1 (ZKG_EINVAL otherwise). */
+/* a <- h. */
+int zkg_quotient(zkg_ctx *ctx, zkg_buf *a, const zkg_buf *b, const zkg_buf *c, uint32_t log_n, const uint32_t *g);
+/* zkg_ntt_forward of data (c's coefficients, already shifted onto the coset), then
+ * data <- (a b - data) / (g^N - 1) with N the transform's size: the quotient runs in the
+ * transform's last pass (forms 2 and 3), saving a kernel and a read and a write of c; the same
+ * words as zkg_ntt_forward followed by zkg_quotient into c. */
+int zkg_ntt_forward_quotient(zkg_ntt *ntt, zkg_buf *data, const zkg_buf *a, const zkg_buf *b, const uint32_t *g);
+
+/* ------------------------------------------------------------------ proving keys (.zkey)
+ * The on-disk form behind zkg_msm_upload_bases_montgomery_256 (Msm::upload_bases_montgomery_256,
+ * src/msm.rs:190-197, documented there as "the form ffjavascript and snarkjs keep points in";
+ * the reference has no reader: its callers parse the file, README.md:104-105). A snarkjs
+ * Groth16 .zkey over BN254 is parsed on the host (no GPU needed); its point sections are then
+ * uploaded as resident MSM bases without conversion. Sections: */
+#define ZKG_ZKEY_IC 3 /* nPublic + 1 G1 points */
+#define ZKG_ZKEY_A 5  /* nVars G1 */
+#define ZKG_ZKEY_B1 6 /* nVars G1 */
+#define ZKG_ZKEY_B2 7 /* nVars G2 */
+#define ZKG_ZKEY_C 8  /* nVars - nPublic - 1 G1 */
+#define ZKG_ZKEY_H 9  /* domainSize G1 */
+typedef struct zkg_zkey zkg_zkey;
+typedef struct {
+  uint32_t protocol; /* 1 = Groth16 */
+  uint32_t n_vars, n_public, domain_size;
+} zkg_zkey_header;
+/* Parses a file image (bytes stay the caller's; the key keeps its own copy of the points).
+ * ZKG_EINVAL with the reason for a malformed file, another protocol, another curve, a section
+ * whose size does not match the header, or a coordinate not below q. */
+int zkg_zkey_parse(const void *bytes, size_t len, zkg_zkey **out);
+void zkg_zkey_free(zkg_zkey *zkey);
+int zkg_zkey_info(const zkg_zkey *zkey, zkg_zkey_header *out);
+/* A point section as the file holds it: 16 (G1) or 32 (G2) words per point, Montgomery form
+ * with R = 2^256, infinity as zeros; *words stays valid until zkg_zkey_free. */
+int zkg_zkey_points(const zkg_zkey *zkey, uint32_t section, const uint32_t **words, size_t *points, int *group);
+/* zkg_msm_upload_bases_montgomery_256 of a point section: resident bases for zkg_msm_run. */
+int zkg_zkey_upload(zkg_ctx *ctx, const zkg_zkey *zkey, uint32_t section, zkg_buf **out);
 
 /* ------------------------------------------------------------------ autotuning
  * No reference counterpart (its parameters are fixed: default_window, item size, TILE_LOG).

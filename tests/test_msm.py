@@ -384,10 +384,12 @@ def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
     assert np.array_equal(got, msm_ref("G1", bases, s))
 
 
+@pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
-def test_sort_aggregation_modes_agree(gpu, mode):
+def test_sort_aggregation_modes_agree(gpu, mode, form):
     """The counting sort's warp aggregation modes (every group / first lane's group / none) on
-    inputs that put many lanes of a warp into one slot and on uniform ones."""
+    inputs that put many lanes of a warp into one slot and on uniform ones, in both sort forms
+    (atomic scatter, ranked placement)."""
     n, c = 20000, 12
     bases = random_points("G1", 960, n)
     cases = [("uniform", scalar_distribution(n, "uniform", 961)), ("sparse", scalar_distribution(n, "sparse", 962)),
@@ -397,5 +399,20 @@ def test_sort_aggregation_modes_agree(gpu, mode):
         for items in (None, 3):
             msm = Msm.with_item_points(gpu, n, c, items) if items else Msm(gpu, n, c)
             msm.set_sort(mode)
+            msm.set_sort_form(form)
             got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, Msm.upload_bases(gpu, bases), gpu.buffer(s)), 32)))
-            assert np.array_equal(got, msm_ref("G1", bases, s)), (name, items, mode)
+            assert np.array_equal(got, msm_ref("G1", bases, s)), (name, items, mode, form)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_slots_beyond_the_rank_field(gpu, form):
+    """More than 65534 entries in one slot (every scalar 1, or r - 1: all points in one bucket of
+    window 0): the ranked sort places the entries past the 16-bit rank through its overflow
+    cursor."""
+    n = (1 << 17) + 3
+    bases = random_points("G1", 970, n)
+    for s in (fr_words([1] * n), fr_words([R - 1] * (n - 5) + [2, 3, 0, 7, R - 2])):
+        msm = Msm(gpu, n, 16)
+        msm.set_sort_form(form)
+        got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, Msm.upload_bases(gpu, bases), gpu.buffer(s)), 32)))
+        assert np.array_equal(got, msm_ref("G1", bases, s)), form

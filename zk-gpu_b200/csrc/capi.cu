@@ -8,6 +8,7 @@
 #include "host_field.hpp"
 #include "msm.hpp"
 #include "ntt.hpp"
+#include "zkey.hpp"
 #include "runtime.hpp"
 #include "server.hpp"
 #include "testing.hpp"
@@ -303,6 +304,58 @@ int zkg_msm_upload_bases_montgomery_256(zkg_ctx* ctx, const uint32_t* xy, size_t
   return upload(ctx, xy, words, true, out);
 }
 
+int zkg_zkey_parse(const void* bytes, size_t len, zkg_zkey** out) {
+  return guard([&] {
+    need(out, "out");
+    *out = nullptr;
+    std::unique_ptr<zkg_zkey> z(new zkg_zkey);
+    z->key = parse_zkey(static_cast<const uint8_t*>(bytes), len);
+    *out = z.release();
+  });
+}
+
+void zkg_zkey_free(zkg_zkey* z) { delete z; }
+
+int zkg_zkey_info(const zkg_zkey* z, zkg_zkey_header* out) {
+  return guard([&] {
+    need(z, "zkey");
+    need(out, "out");
+    out->protocol = z->key.protocol;
+    out->n_vars = z->key.n_vars;
+    out->n_public = z->key.n_public;
+    out->domain_size = z->key.domain_size;
+  });
+}
+
+static const std::vector<uint32_t>& zkey_words(const zkg_zkey* z, uint32_t section) {
+  auto it = z->key.points.find(section);
+  if (zkey_section_group(section) == 0 || it == z->key.points.end())
+    fail(ZKG_EINVAL, "zkey section " + std::to_string(section) + " is not a point section (3, 5, 6, 7, 8, 9)");
+  return it->second;
+}
+
+int zkg_zkey_points(const zkg_zkey* z, uint32_t section, const uint32_t** words, size_t* points, int* group) {
+  return guard([&] {
+    need(z, "zkey");
+    const std::vector<uint32_t>& w = zkey_words(z, section);
+    const int g = zkey_section_group(section);
+    if (words) *words = w.data();
+    if (points) *points = w.size() / (g == ZKG_G1 ? 16 : 32);
+    if (group) *group = g;
+  });
+}
+
+int zkg_zkey_upload(zkg_ctx* ctx, const zkg_zkey* z, uint32_t section, zkg_buf** out) {
+  const zkg_zkey* zz = z;
+  const std::vector<uint32_t>* w = nullptr;
+  int rc = guard([&] {
+    need(zz, "zkey");
+    w = &zkey_words(zz, section);
+  });
+  if (rc != ZKG_OK) return rc;
+  return upload(ctx, w->data(), w->size(), true, out);
+}
+
 int zkg_msm_new(zkg_ctx* ctx, int group, size_t n, uint32_t c, uint32_t item_points, zkg_msm** out) {
   return guard([&] {
     need(ctx, "ctx");
@@ -334,6 +387,14 @@ int zkg_msm_set_sort(zkg_msm* msm, int mode) {
     need(msm, "msm");
     if (mode < 0 || mode > 3) fail(ZKG_EINVAL, "sort aggregation mode must be 0..3");
     msm->plan.sort_agg = mode;
+  });
+}
+
+int zkg_msm_set_sort_form(zkg_msm* msm, int form) {
+  return guard([&] {
+    need(msm, "msm");
+    if (form < 0 || form > 1) fail(ZKG_EINVAL, "sort form must be 0 or 1");
+    msm->plan.sort_form = form;
   });
 }
 
@@ -587,6 +648,54 @@ int zkg_ntt_inverse_coset(zkg_ntt* ntt, zkg_buf* data, zkg_coset* c) {
   });
 }
 
+static void need_elements(const zkg_buf* b, uint32_t log_n, const char* what) {
+  const size_t need_w = (size_t)8 << log_n;
+  if (b->words < need_w)
+    zkg::fail(ZKG_ESIZE, std::string(what) + " buffer holds " + std::to_string(b->words * 4) + " bytes; 2^" +
+                             std::to_string(log_n) + " elements need " + std::to_string(need_w * 4));
+}
+
+int zkg_quotient(zkg_ctx* ctx, zkg_buf* a, const zkg_buf* b, const zkg_buf* c, uint32_t log_n, const uint32_t* g) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(a, "a");
+    need(b, "b");
+    need(c, "c");
+    need(g, "g");
+    if (log_n < 1 || log_n > 28) fail(ZKG_EINVAL, "log_n must be in 1..=28");
+    need_elements(a, log_n, "a");
+    need_elements(b, log_n, "b");
+    need_elements(c, log_n, "c");
+    const host::U256 zinv = coset_zinv(g, log_n);
+    use(ctx);
+    wait_reads(a, ctx->stream);
+    quotient(a->ptr, a->ptr, b->ptr, c->ptr, log_n, zinv, ctx->stream);
+    mark_use(a, ctx->stream);
+    mark_use(b, ctx->stream);
+    mark_use(c, ctx->stream);
+  });
+}
+
+int zkg_ntt_forward_quotient(zkg_ntt* ntt, zkg_buf* data, const zkg_buf* a, const zkg_buf* b, const uint32_t* g) {
+  return guard([&] {
+    need(ntt, "ntt");
+    need(data, "data");
+    need(a, "a");
+    need(b, "b");
+    need(g, "g");
+    const uint32_t log_n = ntt->plan.log_n;
+    need_elements(a, log_n, "a");
+    need_elements(b, log_n, "b");
+    const Quotient q{a->ptr, b->ptr, coset_zinv(g, log_n)};
+    cudaStream_t s = ntt->plan.ctx->stream;
+    wait_reads(data, s);
+    ntt->plan.run(data, false, nullptr, &q);
+    mark_use(data, s);
+    mark_use(a, s);
+    mark_use(b, s);
+  });
+}
+
 int zkg_batch_new(zkg_ctx* ctx, zkg_batch** out) {
   return guard([&] {
     need(ctx, "ctx");
@@ -729,7 +838,7 @@ int zkg_tune_msm(zkg_ctx* ctx, int group, size_t n, const zkg_buf* bases, const 
 int zkg_ntt_set_variant(zkg_ntt* ntt, int variant) {
   return guard([&] {
     need(ntt, "ntt");
-    if (!ntt->plan.set_variant(variant)) fail(ZKG_EINVAL, "NTT variant must be 0 or 1");
+    if (!ntt->plan.set_variant(variant)) fail(ZKG_EINVAL, "NTT variant must be 0..3");
   });
 }
 

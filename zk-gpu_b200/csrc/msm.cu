@@ -85,6 +85,7 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (scan_tiles_n > (uint32_t)kScanTile) fail(ZKG_EINVAL, "too many bucket slots");
   tile_sums.alloc(scan_tiles_n, "msm scan tiles");
   sorted.alloc(max_entries, "msm sorted");
+  if (c <= 16) ranked.alloc(max_entries, "msm ranked digits");
   buckets.alloc(slots * xw, "msm buckets");
 
   heads_max = (max_entries + seg_len - 1) / seg_len;
@@ -159,7 +160,17 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
   switch (which) {
     case kStageCount:
       check_cuda(cudaMemsetAsync(counts.ptr, 0, slots * 4, s), "msm counts clear");
-      if (sort_agg == 1)
+      if (ranked_sort()) {
+        if (sort_agg == 0)
+          msm_rank<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+        else if (sort_agg == 1)
+          msm_rank<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+        else if (sort_agg == 2)
+          msm_rank<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+        else
+          msm_rank<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+        check_launch("msm_rank");
+      } else if (sort_agg == 1)
         msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
       else if (sort_agg == 2)
         msm_count<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
@@ -174,10 +185,17 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("scan_tile_sums");
       scan_tiles<<<1, kScanBlock, 0, s>>>(tile_sums.ptr, scan_tiles_n, slot_start.ptr + slots);
       check_launch("scan_tiles");
-      scan_apply<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr, slot_start.ptr, cursor.ptr);
+      scan_apply<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr, slot_start.ptr, cursor.ptr,
+                                                     ranked_sort() ? kRankOverflow : 0u);
       check_launch("scan_apply");
       break;
     case kStageScatter:
+      if (ranked_sort()) {
+        const dim3 grid((unsigned)grid_for(n, b256), windows);
+        msm_place<<<grid, b256, 0, s>>>(ranked.ptr, n, half, slot_start.ptr, cursor.ptr, sorted.ptr);
+        check_launch("msm_place");
+        break;
+      }
       // every group merged: measured best or equal for the scatter on every distribution
       msm_scatter<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
       check_launch("msm_scatter");

@@ -42,12 +42,18 @@ struct MsmPlan {
   // group of equal slots, 1 = the first lane's group, 2 = none, 3 = the group of the first equal
   // neighbour pair. The scatter pass always merges every group.
   int sort_agg = 3;
+  // Counting sort: 0 = scalar-major scatter through atomic cursors, 1 = ranked (the counting
+  // pass records each digit's rank in its slot, the placing pass runs window by window;
+  // msm_rank / msm_place). 1 is the default where it applies (c <= 16).
+  int sort_form = 1;
+  bool ranked_sort() const { return sort_form == 1 && c <= 16; }
   size_t slots = 0, heads_max = 0;
   uint32_t merge_levels = 0, merge_fan_in = 16, scan_tiles_n = 0;
   ReduceLevels levels;
   std::vector<uint32_t> level_m;
 
   DeviceArray counts, slot_start, cursor, tile_sums, sorted, buckets;
+  DeviceArray ranked;  // the ranked sort's digit and rank per (window, point), window-major
   DeviceArray heads[2], head_keys[2];
   DeviceArray tots, runs[2], window_sums, result;
   zkg_buf result_handle;

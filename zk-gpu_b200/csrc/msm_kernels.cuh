@@ -166,6 +166,65 @@ __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint
   }
 }
 
+// ------------------------------------------------------------------ ranked counting sort
+//
+// The same sort in two passes without scattered stores over the whole sorted array:
+//   msm_rank  recodes each scalar once; the warp-aggregated atomic that counts a digit also
+//             returns its rank within its slot; digit and rank go to a window-major array
+//             (entry w * n + i: bits 0..15 the digit, bucket | sign << 15, 0x7fff for a zero
+//             digit; bits 16..31 the rank, 0xffff when it does not fit) with coalesced stores.
+//   msm_place after the scan, walks the entries window by window: sorted[slot_start + rank] =
+//             point index | sign. A window's slots span ~4n bytes of the sorted array, so the
+//             4-byte stores of the blocks in flight meet in L2 and reach HBM as whole sectors
+//             (the scalar-major scatter touches all windows' ranges at once: 1 GiB at 2^24).
+// Ranks of 0xffff and above (a slot with more than 65534 entries: skewed scalars) are placed
+// through an atomic cursor that starts at slot_start + 0xffff. For c <= 16 (15-bit buckets).
+constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occurs for c <= 16
+constexpr uint32_t kRankOverflow = 0xffffu;
+
+template <int AGG>
+__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
+                         uint32_t* __restrict__ counts, uint32_t* __restrict__ ranked) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < n;
+  Recoder rc;
+  if (live) load_scalar(scalars, i, rc.s);
+  const uint32_t half = 1u << (c - 1);
+  const unsigned lane = threadIdx.x & 31;
+  for (uint32_t w = 0; w < windows; w++) {
+    bool neg = false;
+    const uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
+    const unsigned peers = slot_peers<AGG>(slot);
+    const int leader = peers ? __ffs(peers) - 1 : (int)lane;
+    uint32_t base = 0;
+    if (peers && (int)lane == leader) base = atomicAdd(&counts[slot], (uint32_t)__popc(peers));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (!live) continue;
+    uint32_t code = kRankZero;
+    if (peers) {
+      const uint32_t rank = base + __popc(peers & ((1u << lane) - 1));
+      code = (slot - w * half) | (neg ? 0x8000u : 0u) | (min(rank, kRankOverflow) << 16);
+    }
+    __stcs(ranked + (size_t)w * n + i, code);  // streamed: read once by msm_place
+  }
+}
+
+// Grid (ceil(n / 256), windows): blockIdx.y is the window, so blocks run window by window.
+__global__ void msm_place(const uint32_t* __restrict__ ranked, size_t n, uint32_t half,
+                          const uint32_t* __restrict__ slot_start, uint32_t* __restrict__ overflow_cursor,
+                          uint32_t* __restrict__ sorted) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t w = blockIdx.y;
+  const uint32_t code = __ldcs(ranked + (size_t)w * n + i);
+  const uint32_t digit = code & 0xffffu;
+  if (digit == kRankZero) return;
+  const uint32_t slot = w * half + (digit & 0x7fffu);
+  const uint32_t rank = code >> 16;
+  const uint32_t pos = rank < kRankOverflow ? slot_start[slot] + rank : atomicAdd(&overflow_cursor[slot], 1u);
+  sorted[pos] = (uint32_t)i | ((digit & 0x8000u) ? kNegBit : 0u);
+}
+
 // ------------------------------------------------------------------ scan (3 phases)
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total, uint32_t* warp_sums) {
@@ -230,10 +289,11 @@ __global__ void __launch_bounds__(kScanBlock) scan_tiles(uint32_t* __restrict__ 
   if (threadIdx.x == 0) *grand = total;
 }
 
-// out[i] = exclusive prefix of in; also copies it to out2 (the scatter cursor).
+// out[i] = exclusive prefix of in; also writes it plus out2_bias to out2 (the scatter cursor).
 __global__ void __launch_bounds__(kScanBlock) scan_apply(const uint32_t* __restrict__ in, size_t len,
                                                          const uint32_t* __restrict__ tile_offsets,
-                                                         uint32_t* __restrict__ out, uint32_t* __restrict__ out2) {
+                                                         uint32_t* __restrict__ out, uint32_t* __restrict__ out2,
+                                                         uint32_t out2_bias) {
   __shared__ uint32_t warp_sums[32];
   size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
@@ -249,7 +309,7 @@ __global__ void __launch_bounds__(kScanBlock) scan_apply(const uint32_t* __restr
   for (int k = 0; k < kScanItems; k++) {
     if (base + k < len) {
       out[base + k] = run;
-      out2[base + k] = run;
+      out2[base + k] = run + out2_bias;
     }
     run += v[k];
   }

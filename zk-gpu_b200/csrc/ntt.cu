@@ -248,6 +248,197 @@ __global__ void __launch_bounds__(kNttThreads, 3)
   }
 }
 
+// (a b - c) zinv for plain Fr words, zinv2 = zinv R^2 (the Montgomery form of zinv, times R):
+// u = a b / R, w = c / R, (u - w) zinv R^2 / R = (a b - c) zinv.
+__device__ __forceinline__ Fr quotient_element(const Fr& a, const Fr& b, const Fr& c, const Fr& zinv2) {
+  Fr one = Fr::zero();
+  one.w[0] = 1;
+  return (a * b - c * one) * zinv2;
+}
+
+// ------------------------------------------------------------------ staged-twiddle form
+//
+// The double-precision butterflies with each stage's twiddles copied into shared memory by
+// cp.async during the stage before, from a table laid out in the order the butterflies use
+// them. The pass table holds one block of 2^tl entries per distinct tile (a tile's twiddles
+// depend on its columns j0 = c mod 2^lm only, so D = 2^max(0, lm - lg) blocks serve all tiles):
+// stage st of the pass occupies entries [elems - (elems >> st), elems - (elems >> (st + 1))),
+// 2^(lh + lg) twiddles where butterfly b reads entry b mod 2^(lh + lg); each stage block is
+// stored limb-major (limb k of entry e at k * size + e), five doubles per twiddle, Montgomery
+// form with R = 2^260. The first pass's table is read once per transform (40 bytes per
+// element; its tiles share no twiddles), the later passes' tables are small and stay in L2.
+
+// Builds a pass table: entries D * elems, from the seed tables (w^j = hi[j >> lo_bits] * lo[j & mask]).
+__global__ void ntt_stage_twiddles(const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo,
+                                   uint32_t lo_bits, uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s,
+                                   size_t entries, double* __restrict__ out) {
+  const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= entries) return;
+  const uint32_t elems = 1u << tl, lg = tl - s;
+  const uint32_t tb = (uint32_t)(id >> tl), off = (uint32_t)(id & (elems - 1));
+  const uint32_t v1 = elems - 1 - off;  // stage st holds v1 in [2^(tl-st-1), 2^(tl-st) - 1]
+  const uint32_t st = v1 == 0 ? tl : tl - 1 - (31 - __clz(v1));
+  double* o = out + (size_t)tb * 5 * elems;
+  if (st >= s) {  // padding at the block's end (entries [elems - 2^lg, elems))
+#pragma unroll
+    for (int k = 0; k < 5; k++) o[5 * (size_t)off + k] = 0.0;
+    return;
+  }
+  const uint32_t base = elems - (elems >> st), size = elems >> (st + 1);
+  const uint32_t e = off - base;
+  const uint32_t col = e & ((1u << lg) - 1), r_lo = e >> lg;
+  const uint32_t c = (tb << lg) + col;
+  const uint32_t j0 = c & ((1u << lm) - 1);
+  const uint32_t t = log_n - lm - s + st;
+  const uint32_t idx = ((r_lo << lm) + j0) << t;  // < n/2
+  const Fr w = load_fe<Fr>(hi + 8 * (size_t)(idx >> lo_bits)) * load_fe<Fr>(lo + 8 * (size_t)(idx & ((1u << lo_bits) - 1)));
+  uint32_t words[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) words[i] = w.w[i];
+  const f64::FqD d = f64::fqd_reduce<f64::FrLimbs>(f64::fqd_from_words_x16(words), &g_multiples_of_r);
+#pragma unroll
+  for (int k = 0; k < 5; k++) o[5 * base + k * size + e] = d.l[k];
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Copies stage st's block (5 * size doubles, size = elems >> (st + 1)) into shared memory.
+__device__ __forceinline__ void stage_twiddles_async(double* dst, const double* tblock, uint32_t elems, uint32_t st) {
+  const uint32_t base = elems - (elems >> st), size = elems >> (st + 1);
+  const double* src = tblock + 5 * (size_t)base;
+  // 16-byte chunks; a block of one entry (size 1: the last stage of a single-column tile) is
+  // copied with the following padding double
+  const uint32_t chunks = (5 * size + 1) / 2;
+  for (uint32_t i = threadIdx.x; i < chunks; i += blockDim.x) cp_async16(dst + 2 * i, src + 2 * i);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// One pass as ntt_pass_f64, with staged twiddles (tw: this pass's table, tw_mask = D - 1).
+// Shared memory: the tile (5 * elems doubles) and two twiddle buffers (stage 0, 2, ...: elems/2
+// entries; stage 1, 3, ...: elems/4), 70 KiB for tiles of 2^10 elements.
+template <bool LAST, bool PAIR>
+__global__ void __launch_bounds__(kNttThreads, PAIR ? 2 : 3)
+    ntt_pass_f64s(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const double* __restrict__ tw,
+                  uint32_t tw_mask, uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag,
+                  Fr scale_mont, const uint32_t* __restrict__ sh_hi, const uint32_t* __restrict__ sh_lo,
+                  uint32_t sh_bits, const uint32_t* __restrict__ qa, const uint32_t* __restrict__ qb, Fr qz2) {
+  using namespace f64;
+  extern __shared__ __align__(16) double smem_d[];
+  const MultiplesOf<FrLimbs>* kr = &g_multiples_of_r;
+  const uint32_t lg = tl - s;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t elems = 1u << tl;
+  double* tile_d = smem_d;
+  double* const twbuf0 = smem_d + 5 * elems;                   // stages 0, 2, 4, ...
+  double* const twbuf1 = smem_d + 5 * elems + 5 * (elems >> 1);  // stages 1, 3, 5, ...
+  const double* tblock = tw + (size_t)(tile & tw_mask) * 5 * elems;
+
+  stage_twiddles_async(twbuf0, tblock, elems, 0);
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    const uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    const Fr v = load_fe_cg<Fr>(src + 8 * (size_t)g);
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = v.w[i];
+    FqD d;
+    words_to_limbs(w, d.l);
+    tile_store_d(tile_d, elems, slot, d);
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+
+  const uint32_t half_elems = elems >> 1;
+  for (uint32_t st = 0; st < s; st++) {
+    if (st + 1 < s) stage_twiddles_async((st & 1) ? twbuf0 : twbuf1, tblock, elems, st + 1);
+    const uint32_t lh = s - 1 - st;
+    const uint32_t size = elems >> (st + 1);  // = 2^(lh + lg)
+    const double* twst = (st & 1) ? twbuf1 : twbuf0;
+    if (PAIR && half_elems % (2 * kNttThreads) == 0) {
+      // two butterflies per iteration, loads first: two independent products in flight
+      for (uint32_t b0 = threadIdx.x; b0 < half_elems; b0 += 2 * kNttThreads) {
+        uint32_t sa[2], sb[2];
+        FqD x[2], y[2], w[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const uint32_t b = b0 + k * kNttThreads;
+          const uint32_t col = b & ((1u << lg) - 1);
+          const uint32_t q = b >> lg;
+          const uint32_t r_lo = q & ((1u << lh) - 1);
+          const uint32_t row_a = ((q >> lh) << (lh + 1)) + r_lo;
+          sa[k] = (row_a << lg) + col;
+          sb[k] = sa[k] + (1u << (lh + lg));
+          const uint32_t j0 = ((tile << lg) + col) & ((1u << lm) - 1);
+          const uint32_t e = b & (size - 1);
+          w[k] = (r_lo | j0) != 0
+                     ? FqD{{twst[e], twst[size + e], twst[2 * size + e], twst[3 * size + e], twst[4 * size + e]}}
+                     : fqd_one260();  // a product by one in Montgomery form returns the value, below 2r
+          x[k] = tile_load_d(tile_d, elems, sa[k]);
+          y[k] = tile_load_d(tile_d, elems, sb[k]);
+        }
+        const FqD s0 = fqd_reduce<FrLimbs>(fqd_add(x[0], y[0]), kr);
+        const FqD s1 = fqd_reduce<FrLimbs>(fqd_add(x[1], y[1]), kr);
+        const FqD o0 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x[0], y[0]), w[0]);
+        const FqD o1 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x[1], y[1]), w[1]);
+        tile_store_d(tile_d, elems, sa[0], s0);
+        tile_store_d(tile_d, elems, sa[1], s1);
+        tile_store_d(tile_d, elems, sb[0], o0);
+        tile_store_d(tile_d, elems, sb[1], o1);
+      }
+    } else
+    for (uint32_t b = threadIdx.x; b < half_elems; b += kNttThreads) {
+      const uint32_t col = b & ((1u << lg) - 1);
+      const uint32_t q = b >> lg;
+      const uint32_t r_lo = q & ((1u << lh) - 1);
+      const uint32_t row_a = ((q >> lh) << (lh + 1)) + r_lo;
+      const uint32_t slot_a = (row_a << lg) + col;
+      const uint32_t slot_b = slot_a + (1u << (lh + lg));
+      const uint32_t c = (tile << lg) + col;
+      const uint32_t j0 = c & ((1u << lm) - 1);
+      const FqD x = tile_load_d(tile_d, elems, slot_a);
+      const FqD y = tile_load_d(tile_d, elems, slot_b);
+      tile_store_d(tile_d, elems, slot_a, fqd_reduce<FrLimbs>(fqd_add(x, y), kr));
+      const FqD d = fqd_sub<2, FrLimbs>(x, y);  // (0, 4r)
+      FqD out;
+      if ((r_lo | j0) != 0) {
+        const uint32_t e = b & (size - 1);
+        const FqD wd{{twst[e], twst[size + e], twst[2 * size + e], twst[3 * size + e], twst[4 * size + e]}};
+        out = fqd_mul<FrLimbs>(d, wd);
+      } else {
+        out = fqd_reduce<FrLimbs>(d, kr);
+      }
+      tile_store_d(tile_d, elems, slot_b, out);
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+  }
+
+  const bool shifted = LAST && sh_hi != nullptr;
+  FqD scale;
+  if (scale_flag && !shifted) {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = scale_mont.w[i];
+    scale = fqd_reduce<FrLimbs>(fqd_from_words_x16(w), kr);
+  }
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    FqD v = tile_load_d(tile_d, elems, slot);
+    if (scale_flag && !shifted) v = fqd_mul<FrLimbs>(v, scale);
+    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    if (LAST) g = __brev(g) >> (32 - log_n);
+    Fr out = fr_from_limbs(v);
+    if (shifted) {
+      const Fr gi = load_fe<Fr>(sh_hi + 8 * (size_t)(g >> sh_bits)) *
+                    load_fe<Fr>(sh_lo + 8 * (size_t)(g & ((1u << sh_bits) - 1)));
+      out = out * gi;
+    }
+    if (LAST && qa != nullptr) out = quotient_element(load_fe<Fr>(qa + 8 * (size_t)g), load_fe<Fr>(qb + 8 * (size_t)g), out, qz2);
+    store_fe(dst + 8 * (size_t)g, out);
+  }
+}
+
 static std::vector<uint32_t> powers_words(const host::U256& step, size_t len) {
   const host::Field& f = host::fr();
   std::vector<uint32_t> out(8 * len);
@@ -267,6 +458,15 @@ static void set_pass_smem_limits() {
   check_cuda(cudaFuncSetAttribute(ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
              "ntt smem attribute");
   check_cuda(cudaFuncSetAttribute(ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+             "ntt smem attribute");
+  const int smem_s = (int)((size_t)70 << kTileLogD);  // tile + two twiddle buffers, forms 2 and 3
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64s<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64s<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64s<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64s<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s),
              "ntt smem attribute");
 }
 
@@ -292,10 +492,10 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   set_variant(1);
 }
 
-uint32_t NttPlan::tile_log() const { return variant == 1 ? kTileLogD : kTileLog; }
+uint32_t NttPlan::tile_log() const { return variant != 0 ? kTileLogD : kTileLog; }
 
 bool NttPlan::set_variant(int v) {
-  if (v != 0 && v != 1) return false;
+  if (v < 0 || v > 3) return false;
   if (v == 1 && !fwd_twd.ptr) {  // twiddle limbs on first use of the double-precision form
     const size_t count = (size_t)1 << (log_n - 1);
     use(ctx);
@@ -311,25 +511,54 @@ bool NttPlan::set_variant(int v) {
   }
   variant = v;
   // Pass split: one tile when it fits, else passes of near-equal size, at most 9 stages each
-  // (integer form, tiles of 2^11) or 8 (double-precision form, tiles of 2^10).
-  set_max_stages(v == 1 ? kMaxStagesPerPassD : kMaxStagesPerPass);
+  // (integer form, tiles of 2^11) or 8 (double-precision forms, tiles of 2^10).
+  set_max_stages(v != 0 ? kMaxStagesPerPassD : kMaxStagesPerPass);
   return true;
 }
 
 bool NttPlan::set_max_stages(uint32_t ms) {
   const uint32_t tlog = tile_log();
-  const uint32_t def = variant == 1 ? kMaxStagesPerPassD : kMaxStagesPerPass;
+  const uint32_t def = variant != 0 ? kMaxStagesPerPassD : kMaxStagesPerPass;
   if (ms < 6 || ms > tlog) return false;
+  bool ok = true;
   if (log_n <= tlog) {
     passes.assign(1, log_n);
     max_stages = def;
-    return ms == def;
+    ok = ms == def;
+  } else {
+    max_stages = ms;
+    uint32_t p = (log_n + ms - 1) / ms;
+    passes.clear();
+    for (uint32_t i = 0; i < p; i++) passes.push_back(log_n / p + (i < log_n % p ? 1u : 0u));
   }
-  max_stages = ms;
-  uint32_t p = (log_n + ms - 1) / ms;
-  passes.clear();
-  for (uint32_t i = 0; i < p; i++) passes.push_back(log_n / p + (i < log_n % p ? 1u : 0u));
-  return true;
+  if (variant >= 2) build_stage_tables();
+  return ok;
+}
+
+void NttPlan::build_stage_tables() {
+  use(ctx);
+  const uint32_t tl = log_n < kTileLogD ? log_n : kTileLogD;
+  const uint32_t lo_bits = log_n / 2;  // as build_twiddles: ceil((log_n - 1) / 2)
+  for (int dir = 0; dir < 2; dir++) stage_tw[dir].clear();
+  stage_tw_mask.clear();
+  uint32_t done = 0;
+  for (uint32_t st : passes) {
+    const uint32_t lm = log_n - done - st;
+    const int spare = (int)log_n - (int)done - (int)tl;  // log2 of the distinct tile blocks
+    const size_t blocks = (size_t)1 << (spare > 0 ? spare : 0);
+    const size_t entries = blocks << tl;
+    stage_tw_mask.push_back((uint32_t)(blocks - 1));
+    for (int dir = 0; dir < 2; dir++) {
+      std::unique_ptr<DeviceArray> t(new DeviceArray);
+      t->alloc(10 * entries, "ntt staged twiddles");
+      ntt_stage_twiddles<<<grid_for(entries, 256), 256, 0, ctx->setup>>>(
+          seeds[dir][1].ptr, seeds[dir][0].ptr, lo_bits, log_n, tl, lm, st, entries, t->as<double>());
+      check_launch("ntt_stage_twiddles");
+      stage_tw[dir].push_back(std::move(t));
+    }
+    done += st;
+  }
+  check_cuda(cudaStreamSynchronize(ctx->setup), "ntt staged twiddles");
 }
 
 void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]) {
@@ -383,8 +612,21 @@ const NttPlan::FusedShift* NttPlan::fused_for(const CosetShift& shift) {
 
 void NttPlan::prepare_shift(const CosetShift& shift) { fused_for(shift); }
 
-void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift) {
+void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift, const Quotient* quot) {
   if (shift && !inverse) fail(ZKG_EINVAL, "a fused coset shift follows an inverse transform");
+  if (quot && inverse) fail(ZKG_EINVAL, "a fused quotient follows a forward transform");
+  if (quot && variant < 2) {  // forms without the fused epilogue: the transform, then the kernel
+    enqueue(data, false, s);
+    quotient(data, quot->a, quot->b, data, log_n, quot->zinv, s);
+    return;
+  }
+  const uint32_t* qa = quot ? quot->a : nullptr;
+  const uint32_t* qb = quot ? quot->b : nullptr;
+  Fr qz2;
+  if (quot) {
+    const host::Field& f = host::fr();
+    host::words32(host::to_mont(host::to_mont(quot->zinv, f), f), qz2.w);
+  }
   const FusedShift* fs = shift ? fused_for(*shift) : nullptr;
   const uint32_t* sh_hi = fs ? shift->hi.ptr : nullptr;
   const uint32_t* sh_lo = fs ? fs->lo.ptr : nullptr;
@@ -396,7 +638,7 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
   const uint32_t tlog = tile_log();
   const uint32_t tl = log_n < tlog ? log_n : tlog;
   const unsigned tiles = 1u << (log_n - tl);
-  const size_t smem = variant == 1 ? (size_t)40 << tl : (size_t)32 << tl;
+  const size_t smem = variant >= 2 ? (size_t)70 << tl : variant == 1 ? (size_t)40 << tl : (size_t)32 << tl;
   uint32_t done = 0;
   const size_t np = passes.size();
   for (size_t i = 0; i < np; i++) {
@@ -407,7 +649,21 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
     uint32_t* dst = last ? data : scratch.ptr;
     const int scale_flag = last && inverse;
     size_t ev = timer.enabled ? timer.begin((int)i, s) : 0;
-    if (variant == 1 && last)
+    const double* stw = variant >= 2 ? stage_tw[inverse ? 1 : 0][i]->as<double>() : nullptr;
+    if (variant == 2 && last)
+      ntt_pass_f64s<true, false><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm,
+                                                                  st, scale_flag, scale, sh_hi, sh_lo, sh_bits, qa, qb, qz2);
+    else if (variant == 2)
+      ntt_pass_f64s<false, false><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm,
+                                                                   st, scale_flag, scale, nullptr, nullptr, 0, nullptr, nullptr, qz2);
+    else if (variant == 3 && last)
+      ntt_pass_f64s<true, true><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm,
+                                                                 st, scale_flag, scale, sh_hi, sh_lo, sh_bits, qa, qb, qz2);
+    else if (variant == 3)
+      ntt_pass_f64s<false, true><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm,
+                                                                  st, scale_flag, scale, nullptr, nullptr, 0, nullptr,
+                                                                  nullptr, qz2);
+    else if (variant == 1 && last)
       ntt_pass_f64<true><<<tiles, kNttThreads, smem, s>>>(src, dst, twd, log_n, tl, lm, st, scale_flag, scale, sh_hi,
                                                           sh_lo, sh_bits);
     else if (variant == 1)
@@ -426,14 +682,14 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
   if (timer.enabled) timer.runs++;
 }
 
-void NttPlan::run(zkg_buf* data, bool inverse, const CosetShift* shift) {
+void NttPlan::run(zkg_buf* data, bool inverse, const CosetShift* shift, const Quotient* quot) {
   const size_t need = (size_t)32 << log_n;
   const size_t have = data->words * 4;
   if (have < need)
     fail(ZKG_ESIZE, "data buffer holds " + std::to_string(have) + " bytes; a 2^" + std::to_string(log_n) +
                         " transform needs " + std::to_string(need));
   use(ctx);
-  enqueue(data->ptr, inverse, ctx->stream, shift);
+  enqueue(data->ptr, inverse, ctx->stream, shift, quot);
 }
 
 }  // namespace zkg
@@ -500,24 +756,35 @@ void CosetShift::run(zkg_buf* data) {
 // the vanishing polynomial x^N - 1 evaluated anywhere on that coset). zinv2 holds zinv * R^2
 // (Montgomery form of zinv times R), so three Montgomery products give the plain result:
 //   u = a*b/R, w = c/R, (u - w) * zinv*R^2 / R = (a*b - c) * zinv.
-__global__ void quotient_kernel(uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
-                                const uint32_t* __restrict__ c, size_t n, Fr zinv2) {
+// out may be a or c (each element is read before it is written, by the same thread).
+__global__ void quotient_kernel(uint32_t* out, const uint32_t* a, const uint32_t* __restrict__ b, const uint32_t* c,
+                                size_t n, Fr zinv2) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  Fr one = Fr::zero();
-  one.w[0] = 1;
-  Fr u = load_fe<Fr>(a + 8 * i) * load_fe<Fr>(b + 8 * i);
-  Fr w = load_fe<Fr>(c + 8 * i) * one;
-  store_fe(a + 8 * i, (u - w) * zinv2);
+  const Fr v = quotient_element(load_fe<Fr>(a + 8 * i), load_fe<Fr>(b + 8 * i), load_fe<Fr>(c + 8 * i), zinv2);
+  store_fe(out + 8 * i, v);
 }
 
-void quotient(uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n, const host::U256& zinv, cudaStream_t s) {
+void quotient(uint32_t* out, const uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n,
+              const host::U256& zinv, cudaStream_t s) {
   const host::Field& f = host::fr();
   Fr z2;
   host::words32(host::to_mont(host::to_mont(zinv, f), f), z2.w);
   const size_t n = (size_t)1 << log_n;
-  quotient_kernel<<<grid_for(n, 256), 256, 0, s>>>(a, b, c, n, z2);
+  quotient_kernel<<<grid_for(n, 256), 256, 0, s>>>(out, a, b, c, n, z2);
   check_launch("quotient_kernel");
+}
+
+host::U256 coset_zinv(const uint32_t* g_plain, uint32_t log_n) {
+  const host::Field& f = host::fr();
+  const host::U256 g_raw = host::from_words32(g_plain);
+  if (!(host::geq(f.p, g_raw) && !host::eq(f.p, g_raw))) fail(ZKG_EINVAL, "coset generator must be below r");
+  const host::U256 g = host::to_mont(g_raw, f);
+  const host::U256 gn = host::pow(g, host::U256{{(uint64_t)1 << log_n, 0, 0, 0}}, f);
+  const host::U256 z = host::sub(gn, f.one, f);
+  if (host::eq(z, host::U256{{0, 0, 0, 0}}))
+    fail(ZKG_EINVAL, "g^N = 1: the coset is the subgroup itself and the vanishing polynomial is zero on it");
+  return host::from_mont(host::inverse(z, f), f);
 }
 
 }  // namespace zkg

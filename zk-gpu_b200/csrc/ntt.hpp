@@ -10,6 +10,14 @@ namespace zkg {
 
 struct CosetShift;
 
+// The Groth16 quotient step fused into a forward transform's last pass: the transform's output
+// c_i becomes (a_i b_i - c_i) zinv (a, b: plain Fr words, natural order; zinv a plain value).
+struct Quotient {
+  const uint32_t* a;
+  const uint32_t* b;
+  host::U256 zinv;
+};
+
 struct NttPlan {
   zkg_ctx* ctx;
   uint32_t log_n;
@@ -24,10 +32,11 @@ struct NttPlan {
   StageTimer timer;  // one stage id per pass
 
   NttPlan(zkg_ctx* ctx, uint32_t log_n);
-  // Butterfly form: 0 = 32-bit integer products, 1 = double-precision limbs (the default; on
-  // B200 40% faster than form 0 up to 2^17 elements, 13% at 2^20, within 1% from 2^21 to 2^24;
-  // the tuner times both). Resets the pass split to the
-  // form's default. The first switch to form 1 builds its twiddle limbs (set-up stream, waited for).
+  // Butterfly form: 0 = 32-bit integer products, 1 = double-precision limbs with twiddles read
+  // from a table of w^j, 2 = double-precision limbs with each stage's twiddles staged into shared
+  // memory from per-pass tables in butterfly order. Resets the pass split to the form's default.
+  // The first switch to form 1 builds its twiddle limbs; form 2 builds its tables for each split
+  // (set-up stream, waited for).
   bool set_variant(int variant);
   int variant = 1;
   uint32_t tile_log() const;
@@ -39,8 +48,11 @@ struct NttPlan {
   // the coset shift x_i <- x_i * g^i of that object is applied in the transform's last pass
   // (the same result as the transform followed by shift->enqueue, without another pass over
   // the data); the double-precision form runs the shift as its own kernel.
-  void enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift = nullptr);
-  void run(zkg_buf* data, bool inverse, const CosetShift* shift = nullptr);
+  // With `quot` (forward only), the output is (a b - NTT(data)) zinv instead (fused into the
+  // last pass in forms 2 and 3; the other forms run the quotient kernel after the transform).
+  void enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetShift* shift = nullptr,
+               const Quotient* quot = nullptr);
+  void run(zkg_buf* data, bool inverse, const CosetShift* shift = nullptr, const Quotient* quot = nullptr);
   // Builds (on the set-up stream, then waits) the table a fused shift needs: the shift's
   // low powers times 1/n. enqueue makes it on first use; call this first when enqueue will be
   // captured into a graph.
@@ -48,6 +60,10 @@ struct NttPlan {
 
  private:
   void build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]);
+  // Form 2: one table per pass and direction, for the split in `passes`.
+  void build_stage_tables();
+  std::vector<std::unique_ptr<DeviceArray>> stage_tw[2];
+  std::vector<uint32_t> stage_tw_mask;  // tables' block count - 1, per pass
   struct FusedShift {
     uint64_t serial;
     DeviceArray lo;  // n^-1 g^j, Montgomery form
@@ -67,9 +83,13 @@ struct CosetShift {
   void run(zkg_buf* data);
 };
 
-// a_i <- (a_i * b_i - c_i) * zinv over 2^log_n plain Fr elements (zinv a plain value).
-void quotient(uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n, const host::U256& zinv,
-              cudaStream_t s);
+// out_i <- (a_i * b_i - c_i) * zinv over 2^log_n plain Fr elements (zinv a plain value; out may
+// be a or c).
+void quotient(uint32_t* out, const uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t log_n,
+              const host::U256& zinv, cudaStream_t s);
+// (g^N - 1)^-1 for N = 2^log_n and a plain g < r: the inverse of the vanishing polynomial
+// x^N - 1 anywhere on the coset g*H (ZKG_EINVAL when g^N = 1).
+host::U256 coset_zinv(const uint32_t* g_plain, uint32_t log_n);
 
 }  // namespace zkg
 

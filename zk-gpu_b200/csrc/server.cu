@@ -124,14 +124,6 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
   return msm(32) + msm(64) + ntt + bufs;
 }
 
-// zinv = (g^N - 1)^-1 for the coset g*H of size N (plain value).
-static host::U256 coset_zinv(const uint32_t* g_words, uint32_t log_n) {
-  const host::Field& f = host::fr();
-  host::U256 g = host::to_mont(host::from_words32(g_words), f);
-  host::U256 gn = host::pow(g, host::U256{{(uint64_t)1 << log_n, 0, 0, 0}}, f);
-  host::U256 z = host::sub(gn, f.one, f);
-  return host::from_mont(host::inverse(z, f), f);
-}
 
 std::unique_ptr<ServerSlot> Server::make_slot(uint32_t log_m) {
   use(ctx);
@@ -213,12 +205,14 @@ void Server::enqueue_work(ServerSlot* s, cudaStream_t main, cudaStream_t b0, cud
              "result copy");
   // witness-map chain
   const uint32_t log_n = s->log_m + 1;
-  for (int j = 0; j < 3; j++) {
+  for (int j = 0; j < 3; j++)
     s->ntt->enqueue(s->poly[j].ptr, true, b1, s->shift.get());  // inverse, then shift by g in its last pass
-    s->ntt->enqueue(s->poly[j].ptr, false, b1);
-  }
-  quotient(s->poly[0].ptr, s->poly[1].ptr, s->poly[2].ptr, log_n, coset_zinv(cfg.coset_g, log_n), b1);
-  s->ntt->enqueue(s->poly[0].ptr, true, b1, s->unshift.get());
+  s->ntt->enqueue(s->poly[0].ptr, false, b1);
+  s->ntt->enqueue(s->poly[1].ptr, false, b1);
+  // c's forward transform ends with h = (a b - c) / (g^N - 1), written over c
+  const Quotient q{s->poly[0].ptr, s->poly[1].ptr, coset_zinv(cfg.coset_g, log_n)};
+  s->ntt->enqueue(s->poly[2].ptr, false, b1, nullptr, &q);
+  s->ntt->enqueue(s->poly[2].ptr, true, b1, s->unshift.get());
   if (fork) {
     check_cuda(cudaEventRecord(s->join[0], b0), "join");
     check_cuda(cudaEventRecord(s->join[1], b1), "join");
@@ -264,7 +258,7 @@ void Server::launch(ServerRequest* r, ServerSlot* s) {
     enqueue_work(s, st, st, st);
   }
   check_cuda(cudaMemcpyAsync(d.out_points, s->results.ptr, (3 * 32 + 64) * 4, cudaMemcpyDeviceToHost, st), "results");
-  check_cuda(cudaMemcpyAsync(d.out_h, s->poly[0].ptr, N * 32, cudaMemcpyDeviceToHost, st), "h");
+  check_cuda(cudaMemcpyAsync(d.out_h, s->poly[2].ptr, N * 32, cudaMemcpyDeviceToHost, st), "h");
   check_cuda(cudaLaunchHostFunc(st, on_done, r), "completion callback");
 }
 

@@ -19,8 +19,8 @@ from .batch import Batch
 from .gpu import Buffer, Gpu
 from .group import Group
 from .msm import Msm, xyzz_to_affine, xyzz_to_affine_g2
-from .ntt import CosetShift, Ntt
+from .ntt import CosetShift, Ntt, quotient
 from . import host
 
-__all__ = ["Batch", "Buffer", "CosetShift", "Gpu", "Group", "Msm", "Ntt", "ZkGpuError", "host", "lib", "xyzz_to_affine",
+__all__ = ["Batch", "Buffer", "CosetShift", "Gpu", "Group", "Msm", "Ntt", "ZkGpuError", "host", "lib", "quotient", "xyzz_to_affine",
            "xyzz_to_affine_g2"]

@@ -69,6 +69,15 @@ SIGNATURES = {
     "zkg_msm_group": (ctypes.c_int, [vp]),
     "zkg_msm_set_variant": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_msm_set_sort": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_set_sort_form": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_quotient": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32, u32p]),
+    "zkg_zkey_parse": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(vp)]),
+    "zkg_zkey_free": (None, [vp]),
+    "zkg_zkey_info": (ctypes.c_int, [vp, ctypes.c_void_p]),
+    "zkg_zkey_points": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "zkg_zkey_upload": (ctypes.c_int, [vp, vp, ctypes.c_uint32, ctypes.POINTER(vp)]),
+    "zkg_ntt_forward_quotient": (ctypes.c_int, [vp, vp, vp, vp, u32p]),
     "zkg_msm_params": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_int)]),
     "zkg_msm_run": (ctypes.c_int, [vp, vp, vp, ctypes.POINTER(vp)]),

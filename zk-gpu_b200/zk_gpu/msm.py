@@ -71,6 +71,11 @@ class Msm:
         group, 2 none, 3 the first equal neighbour pair's group."""
         check(lib().zkg_msm_set_sort(self._h, mode))
 
+    def set_sort_form(self, form: int) -> None:
+        """Counting sort: 0 scatter through atomic cursors, 1 ranked placement window by window
+        (default for c <= 16)."""
+        check(lib().zkg_msm_set_sort_form(self._h, form))
+
     def params(self) -> dict:
         c, items, var = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
         check(lib().zkg_msm_params(self._h, ctypes.byref(c), ctypes.byref(items), ctypes.byref(var)))

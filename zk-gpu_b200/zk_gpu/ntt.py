@@ -41,8 +41,15 @@ class Ntt:
         """inverse() then coset.shift() in one call: the shift runs in the inverse's last pass."""
         check(lib().zkg_ntt_inverse_coset(self._h, data.handle, coset.handle))
 
+    def forward_quotient(self, gpu: Gpu, data: Buffer, a: Buffer, b: Buffer, g: int) -> None:
+        """forward() of data (c on the coset g*H), then data <- (a * b - data) / (g^N - 1), the
+        quotient running in the transform's last pass."""
+        check(lib().zkg_ntt_forward_quotient(self._h, data.handle, a.handle, b.handle, _fr_words(g)))
+
     def set_variant(self, variant: int) -> None:
-        """Butterfly form: 0 = 32-bit integer products (default), 1 = double-precision limbs."""
+        """Butterfly form: 0 = 32-bit integer products, 1 = double-precision limbs with twiddles
+        read from a table of powers, 2 = double-precision limbs with each stage's twiddles staged
+        into shared memory, 3 = form 2 with two butterflies per thread step."""
         check(lib().zkg_ntt_set_variant(self._h, variant))
 
     def set_max_stages(self, max_stages: int) -> None:
@@ -63,6 +70,21 @@ class Ntt:
             self.close()
         except Exception:
             pass
+
+
+def _fr_words(v: int):
+    import numpy as np
+
+    from ._lib import u32p
+    words = np.array([(v >> (32 * i)) & 0xFFFFFFFF for i in range(8)], dtype=np.uint32)
+    _fr_words.keep = words  # alive for the call
+    return words.ctypes.data_as(u32p)
+
+
+def quotient(gpu: Gpu, a: Buffer, b: Buffer, c: Buffer, log_n: int, g: int) -> None:
+    """a <- (a * b - c) / (g^N - 1), N = 2^log_n: the pointwise step of a Groth16 witness map on
+    the coset g*H (plain Fr words, natural order)."""
+    check(lib().zkg_quotient(gpu.handle, a.handle, b.handle, c.handle, log_n, _fr_words(g)))
 
 
 class CosetShift:
