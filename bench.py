@@ -448,14 +448,19 @@ SERVING_KEYS = (18, 20, 21, 22)  # resident proving keys, log2 of their sizes
 SERVING_K = (14, 22)             # circuit size m = 2^k, k uniform over these integers
 
 
-def run_configs(gpu, bases, stream, n_max) -> dict:
+def run_configs(gpu, bases, stream, n_max, cpu_too=True) -> dict:
     """Device time of one call at the other sizes of the benchmark configurations (outside the
     timed step; inputs resident; CUDA events on the library stream, best of three after a
     warm-up): G1 MSM 2^16..2^24 with default_window (uniform scalars, and the two skewed
-    distributions at 2^24), G2 MSM 2^18..2^22 (Montgomery-2^256 upload), Fr NTT 2^16..2^26."""
+    distributions at 2^24), G2 MSM 2^18..2^22 (Montgomery-2^256 upload), Fr NTT 2^16..2^26;
+    for C0 (2^16) and C2 (2^18..2^22, three scalar distributions) also the autotuned plan and the
+    CPU restatement of the reference's CPU path on all host threads (one call each)."""
     import torch
 
-    from zk_gpu import Group, Msm, Ntt
+    from oracle import cpu
+    from zk_gpu import Group, Msm, Ntt, xyzz_to_affine
+    from zk_gpu.autotune import tuned_msm
+    from zk_gpu.msm import affine_words
     from zk_gpu.synthetic import generator_multiples, scalar_distribution, uniform_scalars
 
     def device_ms(fn):
@@ -488,6 +493,40 @@ def run_configs(gpu, bases, stream, n_max) -> dict:
         msm.close()
         s.free()
     out["g1_msm_ms"] = g1
+    # C0 and C2 per scalar distribution: default_window, autotuned, and the CPU port
+    threads = os.cpu_count() or 1
+    c2 = {"method": "one call each; GPU: device time, best of 3; autotuned: zkg_tune_msm over windows "
+                    "default-2..default+2, points per thread and accumulation forms, tuned once per size on "
+                    "uniform scalars; cpu: the oracle's C restatement of the reference's CPU MSM on "
+                    f"{threads} host threads, one call, wall time; bit_exact: the GPU results (both plans) "
+                    "equal the CPU result"}
+    host_bases = gpu.read(bases, 16 * min(n_max, 1 << 22)) if cpu_too else None
+    for lg in (16, 18, 20, 22):
+        n = 1 << lg
+        if n > n_max:
+            continue
+        plain = Msm(gpu, n, Msm.default_window(n))
+        su = gpu.buffer(uniform_scalars(n, 1300 + lg))
+        tuned = tuned_msm(gpu, Group.G1, n, bases, su, reps=1)
+        su.free()
+        for kind in ("uniform", "sparse", "r-1") if lg > 16 else ("uniform",):
+            sh = scalar_distribution(n, kind, 1400 + lg)
+            sk = gpu.buffer(sh)
+            row = {"default_window": device_ms(lambda: plain.run(gpu, bases, sk)),
+                   "autotuned": device_ms(lambda: tuned.run(gpu, bases, sk)), "tuned_plan": tuned.params()}
+            if cpu_too:
+                t0 = time.perf_counter()
+                want = cpu.msm("G1", host_bases[: 16 * n], sh, mont256=True, nthreads=threads)
+                row["cpu_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+                got_p = affine_words(xyzz_to_affine(gpu.read(plain.run(gpu, bases, sk), 32)))
+                got_t = affine_words(xyzz_to_affine(gpu.read(tuned.run(gpu, bases, sk), 32)))
+                row["bit_exact"] = bool(np.array_equal(got_p, want) and np.array_equal(got_t, want))
+                row["cpu_over_gpu"] = round(row["cpu_ms"] / row["default_window"], 1)
+            c2[f"2^{lg} {kind}"] = row
+            sk.free()
+        plain.close()
+        tuned.close()
+    out["g1_msm_c0_c2"] = c2
     g2 = {}
     n2 = 1 << 22
     b2 = generator_multiples(gpu, Group.G2, uniform_scalars(n2, 500), mont256=True)
@@ -514,6 +553,63 @@ def run_configs(gpu, bases, stream, n_max) -> dict:
     return out
 
 
+def request_device_ms(gpu, keys, pool) -> dict:
+    """Summed kernel time of one Groth16-shaped request per size class k, measured alone with
+    CUDA events on the library stream through the public API: three G1 MSMs and one G2 MSM on the
+    smallest key that covers m, and the witness-map chain (3 inverse transforms with the coset
+    shift, 2 forward transforms, the forward transform of c with the quotient, the inverse with
+    the unshift); best of 3 after a warm-up."""
+    import torch
+
+    from zk_gpu import CosetShift, Group, Msm, Ntt, lib
+    from oracle import bn254
+
+    stream = torch.cuda.ExternalStream(lib().zkg_ctx_stream(gpu.handle), device=torch.device("cuda", 0))
+    g = 7
+    out = {}
+    for k, req in sorted(pool.items()):
+        m = 1 << k
+        n_key, g1b, g2b = next(key for key in keys if key[0] >= m)
+        m1 = Msm(gpu, m, Msm.default_window(m))
+        m2 = Msm.for_group(gpu, Group.G2, m, Msm.default_window(m))
+        g1_host = [req.g1[j].array.copy() for j in range(3)]
+        for j in range(3):
+            g1_host[j][8 * req.g1_counts[j]:] = 0  # the server zeroes the tail of a shorter vector too
+        s1 = [gpu.buffer(h) for h in g1_host]
+        s2 = gpu.buffer(req.g2.array)
+        polys = [gpu.buffer(req.polys[j].array) for j in range(3)]
+        ntt = Ntt(gpu, k + 1)
+        shift = CosetShift(gpu, k + 1, g)
+        unshift = CosetShift(gpu, k + 1, pow(g, bn254.R - 2, bn254.R))
+
+        def chain():
+            for j in range(3):
+                m1.run(gpu, g1b, s1[j])
+            m2.run(gpu, g2b, s2)
+            for j in range(3):
+                ntt.inverse_coset(gpu, polys[j], shift)
+            ntt.forward(gpu, polys[0])
+            ntt.forward(gpu, polys[1])
+            ntt.forward_quotient(gpu, polys[2], polys[0], polys[1], g)
+            ntt.inverse_coset(gpu, polys[2], unshift)
+
+        chain()
+        best = float("inf")
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            chain()
+            e1.record(stream)
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[k] = best
+        for b in s1 + [s2] + polys:
+            b.free()
+        for o in (m1, m2, ntt, shift, unshift):
+            o.close()
+    return out
+
+
 def run_serving(a, gpu) -> dict:
     """The Groth16-shaped stream through the plain server (one request at a time, operations
     launched one by one) and the served one (lanes, graphs, continuous batching, HBM-budget
@@ -537,6 +633,7 @@ def run_serving(a, gpu) -> dict:
         g1[2] = g1[2][: 8 * (m - 1024)]
         polys = [uniform_scalars(2 * m, 950 + 3 * k + j) for j in range(3)]
         pool[k] = req.fill(g1, uniform_scalars(m, 990 + k), polys)
+    kernel_ms = request_device_ms(gpu, keys, pool)
     rates = [float(r) for r in a.serving_rates.split(",") if r]
     out = {"workload": "Groth16-shaped requests: m = 2^k, k uniform in {14..22}; 3 G1 MSMs (m, m, m-1024) + "
                        "1 G2 MSM (m) on resident keys 2^18/2^20/2^21/2^22 + 7 Fr NTTs of 2m with coset shifts "
@@ -567,11 +664,16 @@ def run_serving(a, gpu) -> dict:
             st1 = servers[mode].stats()
             point[mode] = {key: round(v, 3) for key, v in r.items() if key != "requests"}
             point[mode]["slots_made"] = st1["slots_created"] - st0["slots_created"]
+            # device-busy fraction: the requests' summed kernel time (each measured alone) over
+            # the stream's wall time; near 1, no schedule can serve the mix faster
+            point[mode]["device_busy_frac"] = round(sum(kernel_ms[int(k)] for k in ks) / (r["wall_s"] * 1e3), 3)
             point[mode]["slot_build_ms"] = round(st1["build_ms"] - st0["build_ms"], 1)
         point["throughput_ratio"] = round(point["batched"]["req_per_s"] / point["plain"]["req_per_s"], 3)
         out["points"].append(point)
     for sv in servers.values():
         sv.close()
+    out["request_kernel_ms"] = {f"k={k}": round(v, 3) for k, v in sorted(kernel_ms.items())}
+    out["device_bound_req_per_s"] = round(1e3 * len(kernel_ms) / sum(kernel_ms.values()), 2)
     top = out["points"][-1]
     out["max_rate_ratio"] = top["throughput_ratio"]
     return out
@@ -662,8 +764,9 @@ def run_reference(a, d: Dist) -> dict | None:
 
 def profile_case(msm_form=None, ntt_form=None):
     """The small case the ncu captures in profiles/ run: one Fq product probe launch set, one
-    G1 MSM 2^22 (device-built bases, uniform scalars), one Fr NTT 2^24 forward and one G2 MSM
-    2^20 (device-built bases, Montgomery-2^256 form, uniform scalars)."""
+    G1 MSM 2^22 (device-built bases, uniform scalars), one Fr NTT 2^24 forward, one G2 MSM 2^20
+    (device-built bases, Montgomery-2^256 form, uniform scalars), and a coset shift and a quotient
+    over 2^22 elements."""
     from zk_gpu import Gpu, Group, Msm, Ntt, lib
     from zk_gpu._lib import check
     from zk_gpu.synthetic import generator_multiples, uniform_scalars
@@ -695,6 +798,16 @@ def profile_case(msm_form=None, ntt_form=None):
     s2 = gpu.buffer(uniform_scalars(n2, 5))
     msm2 = Msm.for_group(gpu, Group.G2, n2, Msm.default_window(n2))
     msm2.run(gpu, bases2, s2)
+    gpu.wait()
+    msm2.close()
+    bases2.free()
+    s2.free()
+    # the elementwise kernels of the witness map at 2^22: coset shift and quotient (unfused)
+    from zk_gpu import CosetShift, quotient
+    ln = 22
+    a_, b_, c_ = (gpu.buffer(uniform_scalars(1 << ln, 6 + j)) for j in range(3))
+    CosetShift(gpu, ln, 7).shift(gpu, a_)
+    quotient(gpu, a_, b_, c_, ln, 7)
     gpu.wait()
     print("profile case done", flush=True)
 

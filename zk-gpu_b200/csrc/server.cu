@@ -117,9 +117,13 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
     const size_t B = (size_t)1 << (c - 1), S = (size_t)W * B;
     const size_t entries = (size_t)W * m, L = 8;  // worst case of the automatic segment length
     const size_t heads = entries / L + 1;
-    return 4 * (3 * S + entries + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
+    // counts, slot starts, cursors; sorted and ranked entries; buckets; heads; running sums
+    return 4 * (3 * S + 2 * entries + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
   };
-  const size_t ntt = 32 * N + 2 * 16 * N + 2 * 20 * N;  // scratch, twiddle words and limbs
+  // scratch, twiddle words (both directions), staged twiddle tables (both directions: 40 bytes
+  // per element for the first pass, at most as much again for the later passes' small tables
+  // at these sizes) or the twiddle limbs of form 1 (20 bytes per element per direction)
+  const size_t ntt = 32 * N + 2 * 16 * N + 2 * 48 * N;
   const size_t bufs = 3 * 32 * m + 32 * m + 3 * 32 * N + 4096;
   return msm(32) + msm(64) + ntt + bufs;
 }

@@ -67,7 +67,7 @@ def tuned_msm(gpu: Gpu, group: Group, n: int, bases: Buffer, scalars: Buffer, re
 
 
 def tuned_ntt(gpu: Gpu, log_n: int, data: Buffer, reps: int = 2, refresh: bool = False) -> Ntt:
-    key = f"{gpu.adapter_name}|ntt2|{log_n}"
+    key = f"{gpu.adapter_name}|ntt3|{log_n}"
     cache = _load()
     if refresh or key not in cache:
         var, best, ms = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
