@@ -377,7 +377,7 @@ int zkg_msm_group(const zkg_msm* msm) { return msm ? msm->plan.group : 0; }
 int zkg_msm_set_variant(zkg_msm* msm, int variant) {
   return guard([&] {
     need(msm, "msm");
-    if (variant < 0 || variant > 4) fail(ZKG_EINVAL, "accumulation variant must be 0..4");
+    if (variant < 0 || variant > 6) fail(ZKG_EINVAL, "accumulation variant must be 0..6");
     msm->plan.acc_variant = variant;
   });
 }

@@ -21,8 +21,8 @@ namespace zkg {
 // Dynamic shared memory of msm_accumulate_f64: the G2 form keeps its accumulators there
 // (4 coordinates x 10 doubles x 128 threads); G1 keeps them in registers.
 template <class E>
-static size_t f64_acc_smem() {
-  return std::is_same<E, f64::Fq2D>::value ? (size_t)4 * f64::AccSmem<E>::N * 128 * sizeof(double) : 0;
+static size_t f64_acc_smem(bool smem_acc = std::is_same<E, f64::Fq2D>::value) {
+  return smem_acc ? (size_t)4 * f64::AccSmem<E>::N * 128 * sizeof(double) : 0;
 }
 
 // Allows the G2 form's dynamic shared memory beside its static staging buffers (72 KiB a block).
@@ -201,10 +201,19 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
-      if (acc_variant == 3 || acc_variant == 4) {
+      if ((acc_variant == 5 || acc_variant == 6) && std::is_same<F, Fq>::value) {
+        // G1 with the accumulator in shared memory, four blocks per SM
+        const size_t acc_smem = f64_acc_smem<f64::FqD>(true);
+        if (acc_variant == 5)
+          msm_accumulate_f64<f64::FqD, false, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+        else
+          msm_accumulate_f64<f64::FqD, true, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+      } else if (acc_variant >= 3) {
         using E = typename std::conditional<std::is_same<F, Fq>::value, f64::FqD, f64::Fq2D>::type;
         const size_t acc_smem = f64_acc_smem<E>();
-        if (acc_variant == 3)
+        if (acc_variant == 3 || acc_variant == 6)
           msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
               bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else

@@ -293,8 +293,10 @@ __device__ __forceinline__ bool xyzzd_add_affine(Acc& acc, const E& bx, const E&
 // accumulators in shared memory (AccSmem; in registers they are 80 of them and the kernel
 // spilled): 55.9 / 63.0 ms at 2^22 for one / two products per call, from 67 / 73, still behind
 // the integer pairs (47.3 ms); at three blocks per SM it spills again.
+// G1 with SMEM_ACC (accumulation variants 5 and 6): the accumulator in shared memory as for G2,
+// which frees its 40 registers for a fourth block per SM (128 registers).
 template <class E, bool PAIRS, bool SMEM_ACC = !std::is_same<E, f64::FqD>::value>
-__global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? 3 : 2)
+__global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? (SMEM_ACC ? 4 : 3) : 2)
     msm_accumulate_f64(const uint32_t* __restrict__ bases, const uint32_t* __restrict__ sorted,
                        const uint32_t* __restrict__ slot_start, uint32_t num_slots, uint32_t seg_len,
                        uint32_t* __restrict__ buckets, uint32_t* __restrict__ heads,
