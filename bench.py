@@ -66,10 +66,12 @@ def parse():
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small profiling case (Fq product probe, G1 MSM 2^22, Fr NTT 2^24 forward, "
                          "G2 MSM 2^20) and exit")
-    ap.add_argument("--msm-form", type=int, choices=[0, 1, 2, 3, 4], default=None,
+    ap.add_argument("--msm-form", type=int, choices=[0, 1, 2, 3, 4, 5, 6], default=None,
                     help="profiling case: G1 accumulation form (default: the plan's default)")
-    ap.add_argument("--ntt-form", type=int, choices=[0, 1], default=None,
-                    help="profiling case: NTT butterfly form (0 integer, 1 FP64; default: the plan's default)")
+    ap.add_argument("--ntt-form", type=int, choices=[0, 1, 2, 3], default=None,
+                    help="profiling case: NTT butterfly form (default: the plan's default)")
+    ap.add_argument("--profile-parts", default="g1,ntt,g2,elementwise",
+                    help="profiling case: which parts run (g1, ntt, g2, elementwise), comma-separated")
     return ap.parse_args()
 
 
@@ -762,18 +764,33 @@ def run_reference(a, d: Dist) -> dict | None:
     }
 
 
-def profile_case(msm_form=None, ntt_form=None):
+def profile_case(msm_form=None, ntt_form=None, parts="g1,ntt,g2,elementwise"):
     """The small case the ncu captures in profiles/ run: one Fq product probe launch set, one
     G1 MSM 2^22 (device-built bases, uniform scalars), one Fr NTT 2^24 forward, one G2 MSM 2^20
     (device-built bases, Montgomery-2^256 form, uniform scalars), and a coset shift and a quotient
-    over 2^22 elements."""
-    from zk_gpu import Gpu, Group, Msm, Ntt, lib
+    over 2^22 elements; `parts` selects which of them run."""
+    from zk_gpu import Gpu, lib
     from zk_gpu._lib import check
-    from zk_gpu.synthetic import generator_multiples, uniform_scalars
 
     gpu = Gpu(0)
-    x = ctypes.c_double()
-    check(lib().zkg_bench_integer_pipe(gpu.handle, 3, ctypes.byref(x)))
+    parts = set(parts.split(","))
+    if "g1" in parts:
+        x = ctypes.c_double()
+        check(lib().zkg_bench_integer_pipe(gpu.handle, 3, ctypes.byref(x)))
+        profile_g1(gpu, msm_form)
+    if "ntt" in parts:
+        profile_ntt(gpu, ntt_form)
+    if "g2" in parts:
+        profile_g2(gpu)
+    if "elementwise" in parts:
+        profile_elementwise(gpu)
+    print("profile case done", flush=True)
+
+
+def profile_g1(gpu, msm_form):
+    from zk_gpu import Group, Msm
+    from zk_gpu.synthetic import generator_multiples, uniform_scalars
+
     n = 1 << 22
     bases = generator_multiples(gpu, Group.G1, uniform_scalars(n, 1), mont256=True)
     s = gpu.buffer(uniform_scalars(n, 2))
@@ -785,6 +802,12 @@ def profile_case(msm_form=None, ntt_form=None):
     msm.close()
     bases.free()
     s.free()
+
+
+def profile_ntt(gpu, ntt_form):
+    from zk_gpu import Ntt
+    from zk_gpu.synthetic import uniform_scalars
+
     buf = gpu.buffer(uniform_scalars(1 << 24, 3))
     ntt = Ntt(gpu, 24)
     if ntt_form is not None:
@@ -793,6 +816,12 @@ def profile_case(msm_form=None, ntt_form=None):
     gpu.wait()
     ntt.close()
     buf.free()
+
+
+def profile_g2(gpu):
+    from zk_gpu import Group, Msm
+    from zk_gpu.synthetic import generator_multiples, uniform_scalars
+
     n2 = 1 << 20
     bases2 = generator_multiples(gpu, Group.G2, uniform_scalars(n2, 4), mont256=True)
     s2 = gpu.buffer(uniform_scalars(n2, 5))
@@ -802,20 +831,24 @@ def profile_case(msm_form=None, ntt_form=None):
     msm2.close()
     bases2.free()
     s2.free()
-    # the elementwise kernels of the witness map at 2^22: coset shift and quotient (unfused)
+
+
+def profile_elementwise(gpu):
+    """The elementwise kernels of the witness map at 2^22: coset shift and quotient (unfused)."""
     from zk_gpu import CosetShift, quotient
+    from zk_gpu.synthetic import uniform_scalars
+
     ln = 22
     a_, b_, c_ = (gpu.buffer(uniform_scalars(1 << ln, 6 + j)) for j in range(3))
     CosetShift(gpu, ln, 7).shift(gpu, a_)
     quotient(gpu, a_, b_, c_, ln, 7)
     gpu.wait()
-    print("profile case done", flush=True)
 
 
 def main():
     a = parse()
     if a.profile_case:
-        return profile_case(a.msm_form, a.ntt_form)
+        return profile_case(a.msm_form, a.ntt_form, a.profile_parts)
     d = Dist(a.gpus)
     try:
         out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)
