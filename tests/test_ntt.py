@@ -23,13 +23,27 @@ def test_matches_oracle(gpu, log_n):
     assert np.array_equal(gpu.read(buf, x.size), x), f"inverse NTT did not restore the input at log_n={log_n}"
 
 
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("log_n", [10, 11, 13, 15, 17, 21])
+def test_every_form_matches_oracle(gpu, log_n, form):
+    """Each butterfly form: 0 integer, 1 FP64 with table twiddles, 2 / 3 FP64 with staged
+    twiddles (one / two butterflies per thread step), 4 radix-4 with staged twiddles; sizes with
+    one tile, even and odd stage counts per pass."""
+    x = random_fr(340 + log_n, 1 << log_n)
+    ntt = Ntt(gpu, log_n)
+    ntt.set_variant(form)
+    assert ntt.params()["variant"] == form
+    want = cpu.ntt(x)
+    assert np.array_equal(gpu_ntt(gpu, ntt, x), want), f"log_n={log_n} form={form}"
+    assert np.array_equal(gpu_ntt(gpu, ntt, want, inverse=True), x), f"log_n={log_n} form={form}"
+
+
 @pytest.mark.parametrize("log_n", [10, 11, 13, 16, 20])
 def test_integer_form_matches_oracle(gpu, log_n):
     """The integer butterfly form (variant 0) beside the default double-precision one (which
     every other test of this file runs)."""
     x = random_fr(300 + log_n, 1 << log_n)
     ntt = Ntt(gpu, log_n)
-    assert ntt.params()["variant"] == 1
     ntt.set_variant(0)
     assert ntt.params()["variant"] == 0
     assert np.array_equal(gpu_ntt(gpu, ntt, x), cpu.ntt(x)), f"log_n={log_n}"
@@ -194,7 +208,7 @@ def test_inverse_with_fused_coset_shift(gpu, log_n):
     want_inv = cpu.coset_shift(cpu.ntt(x, True), ginv)
     ntt = Ntt(gpu, log_n)
     shift, unshift = CosetShift(gpu, log_n, COSET_G), CosetShift(gpu, log_n, pow(COSET_G, R - 2, R))
-    for variant in (0, 1):
+    for variant in (0, 1, 2, 3, 4):
         ntt.set_variant(variant)
         for sh, expect in ((shift, want), (unshift, want_inv), (shift, want)):
             buf = gpu.buffer(x)
@@ -227,7 +241,7 @@ def test_every_pass_split_is_exact(gpu, tmp_path, monkeypatch):
     log_n = 20
     x = random_fr(500, 1 << log_n)
     want = cpu.ntt(x)
-    for variant, top in ((0, 11), (1, 10)):
+    for variant, top in ((0, 11), (1, 10), (2, 10), (3, 10), (4, 10)):
         for s in range(6, top + 1):
             ntt = Ntt(gpu, log_n)
             ntt.set_variant(variant)
@@ -250,7 +264,7 @@ def test_plans_of_different_sizes_interleave(gpu):
     big_x, small_x = random_fr(600, 1 << 16), random_fr(601, 1 << 10)
     big = Ntt(gpu, 16)
     small = Ntt(gpu, 10)
-    for variant in (0, 1, 0):
+    for variant in (0, 1, 4, 2, 0, 3):
         big.set_variant(variant)
         small.set_variant(variant)
         assert np.array_equal(gpu_ntt(gpu, big, big_x), cpu.ntt(big_x)), f"variant {variant}"

@@ -32,10 +32,10 @@ def test_quotient_matches_oracle(gpu, log_n):
     assert np.array_equal(gpu.read(ab, a.size), h_ref(a, b, c, g, log_n))
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("log_n", [10, 12, 15])
 def test_forward_quotient_matches_oracle(gpu, log_n, form):
-    """Every butterfly form: 2 and 3 run the quotient in the transform's last pass, 0 and 1 after it."""
+    """Every butterfly form: 2, 3 and 4 run the quotient in the transform's last pass, 0 and 1 after it."""
     n = 1 << log_n
     a, b, c = random_fr(810 + log_n, n), random_fr(811 + log_n, n), random_fr(812 + log_n, n)
     g = 5

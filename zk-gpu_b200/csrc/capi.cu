@@ -838,7 +838,7 @@ int zkg_tune_msm(zkg_ctx* ctx, int group, size_t n, const zkg_buf* bases, const 
 int zkg_ntt_set_variant(zkg_ntt* ntt, int variant) {
   return guard([&] {
     need(ntt, "ntt");
-    if (!ntt->plan.set_variant(variant)) fail(ZKG_EINVAL, "NTT variant must be 0..3");
+    if (!ntt->plan.set_variant(variant)) fail(ZKG_EINVAL, "NTT variant must be 0..4");
   });
 }
 

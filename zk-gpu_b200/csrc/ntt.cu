@@ -316,6 +316,57 @@ __device__ __forceinline__ void stage_twiddles_async(double* dst, const double* 
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+// A tile of a pass into shared memory as limbs (limb-major), from plain words.
+__device__ __forceinline__ void load_tile_f64(const uint32_t* __restrict__ src, double* tile_d, uint32_t tile,
+                                              uint32_t lg, uint32_t lm, uint32_t s, uint32_t elems) {
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    const uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    const Fr v = load_fe_cg<Fr>(src + 8 * (size_t)g);
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = v.w[i];
+    f64::FqD d;
+    f64::words_to_limbs(w, d.l);
+    tile_store_d(tile_d, elems, slot, d);
+  }
+}
+
+// The pass's output: canonical words, in bit-reversed order in the last pass, with the 1/n
+// scaling of an inverse, the fused coset shift (sh_hi != null) or the fused quotient (qa != null).
+template <bool LAST>
+__device__ __forceinline__ void store_tile_f64(uint32_t* __restrict__ dst, const double* tile_d, uint32_t tile,
+                                               uint32_t lg, uint32_t lm, uint32_t s, uint32_t elems, uint32_t log_n,
+                                               int scale_flag, const Fr& scale_mont,
+                                               const uint32_t* __restrict__ sh_hi, const uint32_t* __restrict__ sh_lo,
+                                               uint32_t sh_bits, const uint32_t* __restrict__ qa,
+                                               const uint32_t* __restrict__ qb, const Fr& qz2) {
+  using namespace f64;
+  const MultiplesOf<FrLimbs>* kr = &g_multiples_of_r;
+  const bool shifted = LAST && sh_hi != nullptr;
+  FqD scale;
+  if (scale_flag && !shifted) {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = scale_mont.w[i];
+    scale = fqd_reduce<FrLimbs>(fqd_from_words_x16(w), kr);
+  }
+  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
+    FqD v = tile_load_d(tile_d, elems, slot);
+    if (scale_flag && !shifted) v = fqd_mul<FrLimbs>(v, scale);
+    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
+    if (LAST) g = __brev(g) >> (32 - log_n);
+    Fr out = fr_from_limbs(v);
+    if (shifted) {
+      const Fr gi = load_fe<Fr>(sh_hi + 8 * (size_t)(g >> sh_bits)) *
+                    load_fe<Fr>(sh_lo + 8 * (size_t)(g & ((1u << sh_bits) - 1)));
+      out = out * gi;
+    }
+    if (LAST && qa != nullptr)
+      out = quotient_element(load_fe<Fr>(qa + 8 * (size_t)g), load_fe<Fr>(qb + 8 * (size_t)g), out, qz2);
+    store_fe(dst + 8 * (size_t)g, out);
+  }
+}
+
 // One pass as ntt_pass_f64, with staged twiddles (tw: this pass's table, tw_mask = D - 1).
 // Shared memory: the tile (5 * elems doubles) and two twiddle buffers (stage 0, 2, ...: elems/2
 // entries; stage 1, 3, ...: elems/4), 70 KiB for tiles of 2^10 elements.
@@ -337,16 +388,7 @@ __global__ void __launch_bounds__(kNttThreads, PAIR ? 2 : 3)
   const double* tblock = tw + (size_t)(tile & tw_mask) * 5 * elems;
 
   stage_twiddles_async(twbuf0, tblock, elems, 0);
-  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
-    const uint32_t g = tile_global_index(tile, slot, lg, lm, s);
-    const Fr v = load_fe_cg<Fr>(src + 8 * (size_t)g);
-    uint32_t w[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) w[i] = v.w[i];
-    FqD d;
-    words_to_limbs(w, d.l);
-    tile_store_d(tile_d, elems, slot, d);
-  }
+  load_tile_f64(src, tile_d, tile, lg, lm, s, elems);
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
 
@@ -415,28 +457,98 @@ __global__ void __launch_bounds__(kNttThreads, PAIR ? 2 : 3)
     __syncthreads();
   }
 
-  const bool shifted = LAST && sh_hi != nullptr;
-  FqD scale;
-  if (scale_flag && !shifted) {
-    uint32_t w[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) w[i] = scale_mont.w[i];
-    scale = fqd_reduce<FrLimbs>(fqd_from_words_x16(w), kr);
-  }
-  for (uint32_t slot = threadIdx.x; slot < elems; slot += kNttThreads) {
-    FqD v = tile_load_d(tile_d, elems, slot);
-    if (scale_flag && !shifted) v = fqd_mul<FrLimbs>(v, scale);
-    uint32_t g = tile_global_index(tile, slot, lg, lm, s);
-    if (LAST) g = __brev(g) >> (32 - log_n);
-    Fr out = fr_from_limbs(v);
-    if (shifted) {
-      const Fr gi = load_fe<Fr>(sh_hi + 8 * (size_t)(g >> sh_bits)) *
-                    load_fe<Fr>(sh_lo + 8 * (size_t)(g & ((1u << sh_bits) - 1)));
-      out = out * gi;
+  store_tile_f64<LAST>(dst, tile_d, tile, lg, lm, s, elems, log_n, scale_flag, scale_mont, sh_hi, sh_lo, sh_bits, qa,
+                       qb, qz2);
+}
+
+// Radix-4 form (form 4): the stages of a pass two at a time. A thread takes rows r0, r0 + h/2,
+// r0 + h, r0 + 3h/2 of one column (h = 2^lh the first stage's row distance): the first stage's
+// two butterflies (r0, r0 + h) and (r0 + h/2, r0 + 3h/2), then the second stage's (r0, r0 + h/2)
+// and (r0 + h, r0 + 3h/2), which share one twiddle: four products and three twiddles per four
+// elements, as in two radix-2 stages, with half the shared-memory round trips and barriers. An
+// odd last stage runs as radix-2. Twiddle buffers: two sets, each holding the blocks of one step
+// (stages 0 and 1: 3/4 of a tile's entries; stages 2 and 3: 3/16), the next step's copied in
+// while the current one runs. Shared memory: 40 + 37.5 KiB for tiles of 2^10 elements.
+template <bool LAST>
+__global__ void __launch_bounds__(kNttThreads, 2)
+    ntt_pass_f64r4(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const double* __restrict__ tw,
+                   uint32_t tw_mask, uint32_t log_n, uint32_t tl, uint32_t lm, uint32_t s, int scale_flag,
+                   Fr scale_mont, const uint32_t* __restrict__ sh_hi, const uint32_t* __restrict__ sh_lo,
+                   uint32_t sh_bits, const uint32_t* __restrict__ qa, const uint32_t* __restrict__ qb, Fr qz2) {
+  using namespace f64;
+  extern __shared__ __align__(16) double smem_d[];
+  const MultiplesOf<FrLimbs>* kr = &g_multiples_of_r;
+  const uint32_t lg = tl - s;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t elems = 1u << tl;
+  double* tile_d = smem_d;
+  // set 0: steps 0, 2, ... (first step: stage 0 block of elems/2 entries, stage 1 of elems/4);
+  // set 1: steps 1, 3, ... (stage 2: elems/8, stage 3: elems/16). 5 doubles per entry.
+  double* const set0 = smem_d + 5 * elems;
+  double* const set1 = set0 + 5 * ((elems >> 1) + (elems >> 2));
+  const double* tblock = tw + (size_t)(tile & tw_mask) * 5 * elems;
+  auto copy_step = [&](double* set, uint32_t st) {  // blocks of stages st and st + 1 (when it exists)
+    stage_twiddles_async(set, tblock, elems, st);
+    if (st + 1 < s) stage_twiddles_async(set + 5 * (elems >> (st + 1)), tblock, elems, st + 1);
+  };
+
+  copy_step(set0, 0);
+  load_tile_f64(src, tile_d, tile, lg, lm, s, elems);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+
+  const FqD one = fqd_one260();
+  for (uint32_t st = 0, step = 0; st < s; st += 2, step++) {
+    if (st + 2 < s) copy_step((step & 1) ? set0 : set1, st + 2);
+    const double* twa = (step & 1) ? set1 : set0;
+    const uint32_t lh = s - 1 - st;
+    const uint32_t size_a = elems >> (st + 1);  // = 2^(lh + lg)
+    if (st + 1 < s) {
+      const double* twb = twa + 5 * size_a;
+      const uint32_t size_b = size_a >> 1;
+      const uint32_t hh = 1u << (lh - 1);
+      for (uint32_t u = threadIdx.x; u < (elems >> 2); u += kNttThreads) {
+        const uint32_t col = u & ((1u << lg) - 1);
+        const uint32_t q4 = u >> lg;
+        const uint32_t rr = q4 & (hh - 1);
+        const uint32_t r0 = ((q4 >> (lh - 1)) << (lh + 1)) + rr;
+        const uint32_t j0 = ((tile << lg) + col) & ((1u << lm) - 1);
+        const uint32_t s0 = (r0 << lg) + col, s1 = s0 + (hh << lg), s2 = s0 + (2 * hh << lg),
+                       s3 = s0 + (3 * hh << lg);
+        const uint32_t e0 = (rr << lg) + col, e1 = ((rr + hh) << lg) + col;
+        const bool unit = (rr | j0) == 0;  // twiddle 1 for the first butterfly of each stage
+        const FqD wa0 = unit ? one : FqD{{twa[e0], twa[size_a + e0], twa[2 * size_a + e0], twa[3 * size_a + e0], twa[4 * size_a + e0]}};
+        const FqD wa1{{twa[e1], twa[size_a + e1], twa[2 * size_a + e1], twa[3 * size_a + e1], twa[4 * size_a + e1]}};
+        const FqD wb = unit ? one : FqD{{twb[e0], twb[size_b + e0], twb[2 * size_b + e0], twb[3 * size_b + e0], twb[4 * size_b + e0]}};
+        const FqD x0 = tile_load_d(tile_d, elems, s0), x1 = tile_load_d(tile_d, elems, s1);
+        const FqD x2 = tile_load_d(tile_d, elems, s2), x3 = tile_load_d(tile_d, elems, s3);
+        const FqD y0 = fqd_reduce<FrLimbs>(fqd_add(x0, x2), kr);
+        const FqD y1 = fqd_reduce<FrLimbs>(fqd_add(x1, x3), kr);
+        const FqD y2 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x0, x2), wa0);
+        const FqD y3 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x1, x3), wa1);
+        tile_store_d(tile_d, elems, s0, fqd_reduce<FrLimbs>(fqd_add(y0, y1), kr));
+        tile_store_d(tile_d, elems, s1, fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(y0, y1), wb));
+        tile_store_d(tile_d, elems, s2, fqd_reduce<FrLimbs>(fqd_add(y2, y3), kr));
+        tile_store_d(tile_d, elems, s3, fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(y2, y3), wb));
+      }
+    } else {  // one stage left (lh = 0): radix-2 butterflies of rows (2i, 2i + 1)
+      for (uint32_t b = threadIdx.x; b < (elems >> 1); b += kNttThreads) {
+        const uint32_t col = b & ((1u << lg) - 1);
+        const uint32_t q = b >> lg;
+        const uint32_t slot_a = ((2 * q) << lg) + col, slot_b = slot_a + (1u << lg);
+        const uint32_t j0 = ((tile << lg) + col) & ((1u << lm) - 1);
+        const uint32_t e = b & (size_a - 1);
+        const FqD w = j0 == 0 ? one : FqD{{twa[e], twa[size_a + e], twa[2 * size_a + e], twa[3 * size_a + e], twa[4 * size_a + e]}};
+        const FqD x = tile_load_d(tile_d, elems, slot_a), y = tile_load_d(tile_d, elems, slot_b);
+        tile_store_d(tile_d, elems, slot_a, fqd_reduce<FrLimbs>(fqd_add(x, y), kr));
+        tile_store_d(tile_d, elems, slot_b, fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x, y), w));
+      }
     }
-    if (LAST && qa != nullptr) out = quotient_element(load_fe<Fr>(qa + 8 * (size_t)g), load_fe<Fr>(qb + 8 * (size_t)g), out, qz2);
-    store_fe(dst + 8 * (size_t)g, out);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
   }
+  store_tile_f64<LAST>(dst, tile_d, tile, lg, lm, s, elems, log_n, scale_flag, scale_mont, sh_hi, sh_lo, sh_bits, qa,
+                       qb, qz2);
 }
 
 static std::vector<uint32_t> powers_words(const host::U256& step, size_t len) {
@@ -468,6 +580,11 @@ static void set_pass_smem_limits() {
              "ntt smem attribute");
   check_cuda(cudaFuncSetAttribute(ntt_pass_f64s<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_s),
              "ntt smem attribute");
+  const int smem_r4 = (int)((size_t)80 << kTileLogD);  // tile + two step buffer sets, form 4
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64r4<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_r4),
+             "ntt smem attribute");
+  check_cuda(cudaFuncSetAttribute(ntt_pass_f64r4<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_r4),
+             "ntt smem attribute");
 }
 
 NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
@@ -495,7 +612,7 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
 uint32_t NttPlan::tile_log() const { return variant != 0 ? kTileLogD : kTileLog; }
 
 bool NttPlan::set_variant(int v) {
-  if (v < 0 || v > 3) return false;
+  if (v < 0 || v > 4) return false;
   if (v == 1 && !fwd_twd.ptr) {  // twiddle limbs on first use of the double-precision form
     const size_t count = (size_t)1 << (log_n - 1);
     use(ctx);
@@ -638,7 +755,10 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
   const uint32_t tlog = tile_log();
   const uint32_t tl = log_n < tlog ? log_n : tlog;
   const unsigned tiles = 1u << (log_n - tl);
-  const size_t smem = variant >= 2 ? (size_t)70 << tl : variant == 1 ? (size_t)40 << tl : (size_t)32 << tl;
+  const size_t smem = variant == 4   ? (size_t)80 << tl
+                      : variant >= 2 ? (size_t)70 << tl
+                      : variant == 1 ? (size_t)40 << tl
+                                     : (size_t)32 << tl;
   uint32_t done = 0;
   const size_t np = passes.size();
   for (size_t i = 0; i < np; i++) {
@@ -650,7 +770,14 @@ void NttPlan::enqueue(uint32_t* data, bool inverse, cudaStream_t s, const CosetS
     const int scale_flag = last && inverse;
     size_t ev = timer.enabled ? timer.begin((int)i, s) : 0;
     const double* stw = variant >= 2 ? stage_tw[inverse ? 1 : 0][i]->as<double>() : nullptr;
-    if (variant == 2 && last)
+    if (variant == 4 && last)
+      ntt_pass_f64r4<true><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm, st,
+                                                            scale_flag, scale, sh_hi, sh_lo, sh_bits, qa, qb, qz2);
+    else if (variant == 4)
+      ntt_pass_f64r4<false><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm, st,
+                                                             scale_flag, scale, nullptr, nullptr, 0, nullptr, nullptr,
+                                                             qz2);
+    else if (variant == 2 && last)
       ntt_pass_f64s<true, false><<<tiles, kNttThreads, smem, s>>>(src, dst, stw, stage_tw_mask[i], log_n, tl, lm,
                                                                   st, scale_flag, scale, sh_hi, sh_lo, sh_bits, qa, qb, qz2);
     else if (variant == 2)

@@ -73,7 +73,7 @@ std::vector<NttChoice> tune_ntt(zkg_ctx* ctx, uint32_t log_n, zkg_buf* data, int
   std::unique_ptr<NttPlan> plan(new NttPlan(ctx, log_n));
   if (data->words < ((size_t)8 << log_n)) fail(ZKG_ESIZE, "data buffer too small for the transform");
   std::vector<NttChoice> out;
-  for (int v = 0; v <= 3; v++) {
+  for (int v = 0; v <= 4; v++) {
     plan->set_variant(v);
     const uint32_t tlog = plan->tile_log();
     for (uint32_t s = 6; s <= tlog; s++) {
