@@ -517,17 +517,20 @@ __global__ void __launch_bounds__(kNttThreads, 2)
                        s3 = s0 + (3 * hh << lg);
         const uint32_t e0 = (rr << lg) + col, e1 = ((rr + hh) << lg) + col;
         const bool unit = (rr | j0) == 0;  // twiddle 1 for the first butterfly of each stage
+        // Bounds: tile values below 2r. The first stage's sums stay unreduced (below 4r): the
+        // second stage reduces their sum (below 8r) and multiplies their difference (plus 4r,
+        // below 8r), both within what fqd_reduce (16r) and the product (below 2r out) take.
+        const FqD x0 = tile_load_d(tile_d, elems, s0), x2 = tile_load_d(tile_d, elems, s2);
         const FqD wa0 = unit ? one : FqD{{twa[e0], twa[size_a + e0], twa[2 * size_a + e0], twa[3 * size_a + e0], twa[4 * size_a + e0]}};
-        const FqD wa1{{twa[e1], twa[size_a + e1], twa[2 * size_a + e1], twa[3 * size_a + e1], twa[4 * size_a + e1]}};
-        const FqD wb = unit ? one : FqD{{twb[e0], twb[size_b + e0], twb[2 * size_b + e0], twb[3 * size_b + e0], twb[4 * size_b + e0]}};
-        const FqD x0 = tile_load_d(tile_d, elems, s0), x1 = tile_load_d(tile_d, elems, s1);
-        const FqD x2 = tile_load_d(tile_d, elems, s2), x3 = tile_load_d(tile_d, elems, s3);
-        const FqD y0 = fqd_reduce<FrLimbs>(fqd_add(x0, x2), kr);
-        const FqD y1 = fqd_reduce<FrLimbs>(fqd_add(x1, x3), kr);
+        const FqD y0 = fqd_add(x0, x2);
         const FqD y2 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x0, x2), wa0);
+        const FqD x1 = tile_load_d(tile_d, elems, s1), x3 = tile_load_d(tile_d, elems, s3);
+        const FqD wa1{{twa[e1], twa[size_a + e1], twa[2 * size_a + e1], twa[3 * size_a + e1], twa[4 * size_a + e1]}};
+        const FqD y1 = fqd_add(x1, x3);
         const FqD y3 = fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(x1, x3), wa1);
+        const FqD wb = unit ? one : FqD{{twb[e0], twb[size_b + e0], twb[2 * size_b + e0], twb[3 * size_b + e0], twb[4 * size_b + e0]}};
         tile_store_d(tile_d, elems, s0, fqd_reduce<FrLimbs>(fqd_add(y0, y1), kr));
-        tile_store_d(tile_d, elems, s1, fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(y0, y1), wb));
+        tile_store_d(tile_d, elems, s1, fqd_mul<FrLimbs>(fqd_sub<4, FrLimbs>(y0, y1), wb));
         tile_store_d(tile_d, elems, s2, fqd_reduce<FrLimbs>(fqd_add(y2, y3), kr));
         tile_store_d(tile_d, elems, s3, fqd_mul<FrLimbs>(fqd_sub<2, FrLimbs>(y2, y3), wb));
       }
