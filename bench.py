@@ -44,9 +44,11 @@ MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
 # first pass captured on the 2^24 transform.
 NCU_TRAFFIC = {
     "msm_accumulate_2^24": 28.2e9,
-    "ntt_pass_2^24": 1.96e9,
-    "ntt_pass_f64_2^24": 2.18e9,
+    "ntt_form0_2^24": 1.96e9,
+    "ntt_form1_2^24": 2.18e9,
 }
+# The pass kernel of each NTT form.
+NTT_KERNEL = {0: "ntt_pass", 1: "ntt_pass_f64", 2: "ntt_pass_f64s", 3: "ntt_pass_f64s", 4: "ntt_pass_f64r4"}
 
 
 def parse():
@@ -349,6 +351,7 @@ def run_ours(a, d: Dist) -> dict | None:
     n_pass = len(stn)
     ntt_pass_ms = sum(stn.values()) / max(n_pass, 1)  # mean pass duration (forward and inverse)
     ntt_bytes = 64 * nn  # each pass reads and writes 32 B per element
+    ntt_products = a.log_ntt * nn // 2 - (nn - 1)  # butterflies with a twiddle other than 1
     hbm_peak = None
     try:
         hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
@@ -402,17 +405,27 @@ def run_ours(a, d: Dist) -> dict | None:
                           "algorithmic": f"{FP64_PER_MULMOD} FP64 instructions per Fq product"},
         },
         "roofline_ntt": {
-            "kernel": (f"ntt_pass_f64 (Fr NTT 2^{a.log_ntt}, {n_pass} passes; butterflies in FP64 limbs)"
-                       if ntt.params()["variant"] == 1 else f"ntt_pass (Fr NTT 2^{a.log_ntt}, {n_pass} passes)"),
+            "kernel": (f"{NTT_KERNEL.get(ntt.params()['variant'], 'ntt_pass')} (Fr NTT 2^{a.log_ntt}, {n_pass} passes, "
+                       f"form {ntt.params()['variant']})"),
             "bound": "hbm",
             "achieved": round(ntt_gbs, 1),
             "peak": hbm_peak,
             "unit": "GB/s",
             "frac": round(ntt_gbs / hbm_peak, 4),
             "peak_source": hbm_src,
-            "traffic": NCU_TRAFFIC["ntt_pass_f64_2^24" if ntt.params()["variant"] == 1 else "ntt_pass_2^24"],
-            "algorithmic": "64 B per element per pass (read + write)",
+            "traffic": NCU_TRAFFIC.get(f"ntt_form{ntt.params()['variant']}_2^24"),
+            "algorithmic": "64 B per element per pass (read + write); the first pass also reads its staged "
+                           "twiddles, 40 B per element (form 2)",
             "transform_frac_of_hbm": round((ntt_bytes * n_pass / (sum(stn.values()) * 1e-3) / 1e9) / hbm_peak, 4),
+            "product_rate": {
+                "achieved": round(ntt_products / (sum(stn.values()) / 2 * 1e-3) / 1e9, 2),
+                "peak": round(peaks["fq_mulmod_fp64"] / 1e9, 2),
+                "unit": "G Fr products/s",
+                "frac": round(ntt_products / (sum(stn.values()) / 2 * 1e-3) / peaks["fq_mulmod_fp64"], 4),
+                "algorithmic": f"{ntt_products} twiddle products per forward transform (log2(n) n/2 butterflies "
+                               "less the n - 1 with twiddle 1); peak: the measured rate of independent "
+                               "double-precision-limb Montgomery products (zkg_bench_integer_pipe variant 11)",
+            },
         },
         "integer_pipe_probe": {k: round(v / 1e12, 3) for k, v in peaks.items()},
         "e2e": {

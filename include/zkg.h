@@ -136,6 +136,17 @@ int zkg_msm_set_sort(zkg_msm *msm, int mode);
  * rank within its slot, and the placing pass writes the entries window by window, so the
  * stores of one window meet in L2 (default; applies for c <= 16, larger c use 0). */
 int zkg_msm_set_sort_form(zkg_msm *msm, int form);
+/* Fixed-base MSM over a resident key (no reference counterpart: the reference combines its
+ * windows by Horner, msm_combine.wgsl:13-22, on every run). zkg_msm_fixed_base_table builds, once
+ * per key and window size c, a table of ceil(255/c) rows of n points, row w holding 2^(c w) P_i
+ * (affine, Montgomery form, infinity as zeros; the bases as zkg_msm_upload_bases* made them).
+ * A plan with zkg_msm_set_fixed_base(msm, 1) then takes that table as its `bases`: the digits of
+ * every window go to one set of 2^(c-1) buckets (point w * n + i of the table), so a run has one
+ * bucket reduction instead of one per window and no doublings between windows; the result is
+ * the same point as the plain MSM over the key. Needs c <= 16 and windows * n < 2^31; the
+ * table holds windows times the key's memory. */
+int zkg_msm_fixed_base_table(zkg_ctx *ctx, int group, const zkg_buf *bases, size_t n, uint32_t c, zkg_buf **out);
+int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,

@@ -8,7 +8,7 @@ import pytest
 
 from common import fr_words, gpu_msm, msm_ref, quick, random_fr, random_points
 from oracle import bn254, cpu
-from zk_gpu import Group, Msm, xyzz_to_affine
+from zk_gpu import Group, Msm, xyzz_to_affine, xyzz_to_affine_g2
 from zk_gpu.msm import affine_words
 from zk_gpu.synthetic import generator_multiples, infinity_mask, scalar_distribution, uniform_scalars
 
@@ -416,3 +416,51 @@ def test_slots_beyond_the_rank_field(gpu, form):
         msm.set_sort_form(form)
         got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, Msm.upload_bases(gpu, bases), gpu.buffer(s)), 32)))
         assert np.array_equal(got, msm_ref("G1", bases, s)), form
+
+
+@pytest.mark.parametrize("group", ["G1", "G2"])
+def test_fixed_base_tables(gpu, group):
+    """A plan in fixed-base mode over the table of 2^(c w) P_i gives the plain MSM's point: every
+    window's digits in one set of buckets, no combination. Window sizes 9..16, points at infinity,
+    and scalars 0, 1, r - 1 and window-boundary values (whose signed digits carry into the next
+    window) beside uniform ones; table rows spot-checked against the oracle."""
+    grp = Group.G1 if group == "G1" else Group.G2
+    n = 1500
+    bases = random_points(group, 980, n)
+    aw = grp.affine_words()
+    bases[: aw * 3] = 0  # three points at infinity
+    base_buf = Msm.upload_bases(gpu, bases)
+    special = [0, 1, R - 1, (1 << 15) - 1, 1 << 15, (1 << 16) + (1 << 15), R - (1 << 20)]
+    for c in (9, 11, 13, 16):
+        table = Msm.fixed_base_table(gpu, grp, base_buf, n, c)
+        windows = (255 + c - 1) // c
+        if c == 11:  # rows: 2^(c w) P_i for a few (w, i)
+            words = gpu.read(table, windows * n * aw)
+            for w, i in ((0, 5), (1, 7), (windows - 1, 9)):
+                row = words[(w * n + i) * aw: (w * n + i + 1) * aw]
+                want = cpu.scalar_mul(group, bases[i * aw: (i + 1) * aw], np.array(bn254.words32(pow(2, c * w, R)),
+                                                                                   dtype=np.uint32))
+                assert np.array_equal(cpu.fq_to_mont256(want), row), (w, i)
+        for seed in (0, 1):
+            s = random_fr(990 + c + seed, n).reshape(n, 8)
+            if seed:
+                for j, v in enumerate(special):
+                    s[j] = bn254.words32(v)
+            s = s.reshape(-1)
+            msm = Msm.for_group(gpu, grp, n, c)
+            msm.set_fixed_base(True)
+            words = gpu.read(msm.run(gpu, table, gpu.buffer(s)), grp.xyzz_words())
+            conv = xyzz_to_affine if grp == Group.G1 else xyzz_to_affine_g2
+            assert np.array_equal(affine_words(conv(words), grp), msm_ref(group, bases, s)), (group, c, seed)
+
+
+def test_fixed_base_checks(gpu):
+    n = 64
+    bases = Msm.upload_bases(gpu, random_points("G1", 985, n))
+    msm = Msm(gpu, n, 17)
+    with pytest.raises(Exception, match="c <= 16"):
+        msm.set_fixed_base(True)
+    msm = Msm(gpu, n, 12)
+    msm.set_fixed_base(True)
+    with pytest.raises(Exception, match="bases buffer holds"):
+        msm.run(gpu, bases, gpu.buffer(random_fr(986, n)))  # the key itself, not its table

@@ -398,6 +398,36 @@ int zkg_msm_set_sort_form(zkg_msm* msm, int form) {
   });
 }
 
+int zkg_msm_fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, uint32_t c, zkg_buf** out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(bases, "bases");
+    need(out, "out");
+    *out = nullptr;
+    const uint32_t windows = c >= 1 ? (255 + c - 1) / c : 0;
+    const size_t aw = group == ZKG_G2 ? 32 : 16;
+    use(ctx);
+    zkg_buf* b = new_buffer(ctx, (size_t)windows * n * aw);
+    try {
+      wait_reads(b, ctx->stream);
+      fixed_base_table(ctx, group, bases, n, c, b);
+      mark_use(bases, ctx->stream);
+      mark_use(b, ctx->stream);
+    } catch (...) {
+      zkg_buf_free(b);
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int zkg_msm_set_fixed_base(zkg_msm* msm, int enable) {
+  return guard([&] {
+    need(msm, "msm");
+    msm->plan.set_fixed_base(enable != 0);
+  });
+}
+
 int zkg_msm_params(const zkg_msm* msm, uint32_t* c, uint32_t* item_points, int* variant) {
   return guard([&] {
     need(msm, "msm");

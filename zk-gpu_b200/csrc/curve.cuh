@@ -119,6 +119,35 @@ __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) 
   return Xyzz<F>{x3, t - sppp, zz3, zzz3};
 }
 
+// ------------------------------------------------------------------ inversion (Fermat)
+
+// a^(p-2) mod p, square-and-multiply over the exponent bits from the top (a != 0).
+template <class P>
+__device__ Fp<P> fp_inverse(const Fp<P>& a) {
+  const uint32_t e[8] = {P::P0 - 2u, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};  // p0 >= 2
+  Fp<P> acc = Fp<P>::one();
+  for (int bit = 255; bit >= 0; bit--) {
+    acc = acc * acc;
+    if ((e[bit >> 5] >> (bit & 31)) & 1) acc = acc * a;
+  }
+  return acc;
+}
+
+static __device__ Fq field_inverse(const Fq& a) { return fp_inverse(a); }
+// 1 / (a + bu) = (a - bu) / (a^2 + b^2)
+static __device__ Fq2 field_inverse(const Fq2& x) {
+  Fq inv = fp_inverse(x.a * x.a + x.b * x.b);
+  return Fq2{x.a * inv, neg(x.b * inv)};
+}
+
+// XYZZ -> affine with one inversion: I = 1/(ZZ*ZZZ), 1/ZZ = ZZZ*I, 1/ZZZ = ZZ*I.
+template <class F>
+__device__ Affine<F> to_affine(const Xyzz<F>& p) {
+  if (is_infinity(p)) return Affine<F>{F::zero(), F::zero()};
+  F inv = field_inverse(p.zz * p.zzz);
+  return Affine<F>{p.x * (p.zzz * inv), p.y * (p.zz * inv)};
+}
+
 // ------------------------------------------------------------------ memory format
 // Affine: x then y (FieldWords each); XYZZ: x, y, zz, zzz. Montgomery form, R = 2^256.
 

@@ -271,6 +271,11 @@ __device__ __forceinline__ FqD fqd_one256() {
   return FqD{{(double)0xd438dc58f0d9dull, (double)0x28f5c70b3dd35ull, (double)0x879462c0a78ebull,
               (double)0xdf2f666ea36f7ull, (double)0xe0a77c19a07ull}};
 }
+// One in R = 2^260 Montgomery form for Fr (2^260 mod r), the NTT's unit twiddle.
+__device__ __forceinline__ FqD frd_one260() {
+  return FqD{{(double)0xb6b753fffffacull, (double)0x380f271055b9dull, (double)0x18f016ecef7c8ull,
+              (double)0x724f85a9201d8ull, (double)0x1f16424e1bb7ull}};
+}
 __device__ __forceinline__ FqD fqd_one260() {
   return FqD{{(double)0x20880f6fce4b4ull, (double)0x49baa989a8455ull, (double)0x18f014a498908ull,
               (double)0x724f85a9201d8ull, (double)0x1f16424e1bb7ull}};

@@ -148,10 +148,34 @@ void MsmPlan::check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const 
   if (sb < need_s)
     fail(ZKG_ESIZE, "scalars buffer holds " + std::to_string(sb) + " bytes; " + std::to_string(n) +
                         " scalars need " + std::to_string(need_s));
-  size_t bb = bases->words * 4, need_b = n * affine_words() * 4;
+  const size_t points = fixed_base ? (size_t)windows * n : n;  // a fixed-base table has a row per window
+  size_t bb = bases->words * 4, need_b = points * affine_words() * 4;
   if (bb < need_b)
-    fail(ZKG_ESIZE, "bases buffer holds " + std::to_string(bb) + " bytes; " + std::to_string(n) + " points need " +
-                        std::to_string(need_b));
+    fail(ZKG_ESIZE, "bases buffer holds " + std::to_string(bb) + " bytes; " + std::to_string(points) +
+                        " points need " + std::to_string(need_b));
+}
+
+void MsmPlan::set_fixed_base(bool enable) {
+  if (enable && c > 16) fail(ZKG_EINVAL, "fixed-base tables need a window size c <= 16, got " + std::to_string(c));
+  if (enable && (size_t)windows * n >= (size_t)kNegBit)
+    fail(ZKG_EINVAL, "a fixed-base table holds fewer than 2^31 points");
+  fixed_base = enable;
+}
+
+void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, uint32_t c, zkg_buf* out) {
+  if (n < 1) fail(ZKG_EINVAL, "an MSM needs at least one point");
+  if (c < 9 || c > 20) fail(ZKG_EINVAL, "window size c must be in 9..=20, got " + std::to_string(c));
+  if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+  const uint32_t windows = (255 + c - 1) / c;
+  const size_t aw = group == ZKG_G1 ? 16 : 32;
+  if (bases->words < n * aw) fail(ZKG_ESIZE, "bases buffer too small for n points");
+  if (out->words < (size_t)windows * n * aw) fail(ZKG_ESIZE, "table buffer too small for windows * n points");
+  use(ctx);
+  if (group == ZKG_G1)
+    msm_fixed_base_table<Fq><<<grid_for(n, 128), 128, 0, ctx->stream>>>(bases->ptr, n, c, windows, out->ptr);
+  else
+    msm_fixed_base_table<Fq2><<<grid_for(n, 128), 128, 0, ctx->stream>>>(bases->ptr, n, c, windows, out->ptr);
+  check_launch("msm_fixed_base_table");
 }
 
 template <class F>
@@ -159,16 +183,20 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
   const unsigned b256 = 256;
   switch (which) {
     case kStageCount:
-      check_cuda(cudaMemsetAsync(counts.ptr, 0, slots * 4, s), "msm counts clear");
+      check_cuda(cudaMemsetAsync(counts.ptr, 0, active_slots() * 4, s), "msm counts clear");
       if (ranked_sort()) {
         if (sort_agg == 0)
-          msm_rank<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+          msm_rank<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
+                                                                ranked.ptr);
         else if (sort_agg == 1)
-          msm_rank<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+          msm_rank<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
+                                                                ranked.ptr);
         else if (sort_agg == 2)
-          msm_rank<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+          msm_rank<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
+                                                                ranked.ptr);
         else
-          msm_rank<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr, ranked.ptr);
+          msm_rank<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
+                                                                ranked.ptr);
         check_launch("msm_rank");
       } else if (sort_agg == 1)
         msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
@@ -181,18 +209,22 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_count");
       break;
     case kStageScan:
-      scan_tile_sums<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr);
+    {
+      const size_t ns = active_slots();
+      const uint32_t tiles = (uint32_t)((ns + kScanTile - 1) / kScanTile);
+      scan_tile_sums<<<tiles, kScanBlock, 0, s>>>(counts.ptr, ns, tile_sums.ptr);
       check_launch("scan_tile_sums");
-      scan_tiles<<<1, kScanBlock, 0, s>>>(tile_sums.ptr, scan_tiles_n, slot_start.ptr + slots);
+      scan_tiles<<<1, kScanBlock, 0, s>>>(tile_sums.ptr, tiles, slot_start.ptr + ns);
       check_launch("scan_tiles");
-      scan_apply<<<scan_tiles_n, kScanBlock, 0, s>>>(counts.ptr, slots, tile_sums.ptr, slot_start.ptr, cursor.ptr,
+      scan_apply<<<tiles, kScanBlock, 0, s>>>(counts.ptr, ns, tile_sums.ptr, slot_start.ptr, cursor.ptr,
                                                      ranked_sort() ? kRankOverflow : 0u);
       check_launch("scan_apply");
       break;
+    }
     case kStageScatter:
       if (ranked_sort()) {
         const dim3 grid((unsigned)grid_for(n, b256), windows);
-        msm_place<<<grid, b256, 0, s>>>(ranked.ptr, n, half, slot_start.ptr, cursor.ptr, sorted.ptr);
+        msm_place<<<grid, b256, 0, s>>>(ranked.ptr, n, half, fixed_base, slot_start.ptr, cursor.ptr, sorted.ptr);
         check_launch("msm_place");
         break;
       }
@@ -206,35 +238,37 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
         const size_t acc_smem = f64_acc_smem<f64::FqD>(true);
         if (acc_variant == 5)
           msm_accumulate_f64<f64::FqD, false, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else
           msm_accumulate_f64<f64::FqD, true, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       } else if (acc_variant >= 3) {
         using E = typename std::conditional<std::is_same<F, Fq>::value, f64::FqD, f64::Fq2D>::type;
         const size_t acc_smem = f64_acc_smem<E>();
         if (acc_variant == 3 || acc_variant == 6)
           msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else
           msm_accumulate_f64<E, false><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       }
       else if (acc_variant == 1)
         msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else if (acc_variant == 2)
         msm_accumulate<typename PairedOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)slots, seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+            bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else
-        msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr, (uint32_t)slots,
+        msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr,
+                                                                   (uint32_t)active_slots(),
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
     case kStageCombine:
       // c (W - 1) dependent doublings: one warp, each level's independent products on separate
       // lanes (one out-of-line product per lane).
-      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, windows, c, result.ptr);
+      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), c,
+                                                                       result.ptr);
       check_launch("msm_combine_lanes");
       break;
     case kStageMerge:
@@ -255,7 +289,7 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
       for (uint32_t l = 0; l < merge_levels; l++) {
         size_t out_len = (len + merge_fan_in - 1) / merge_fan_in;
         int src = l & 1, dst = src ^ 1;
-        msm_merge<FC><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)slots, seg_len, merge_fan_in, l,
+        msm_merge<FC><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)active_slots(), seg_len, merge_fan_in, l,
                                                             heads[src].ptr, head_keys[src].ptr, heads[dst].ptr,
                                                             head_keys[dst].ptr, buckets.ptr);
         check_launch("msm_merge");
@@ -270,7 +304,7 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
         uint32_t m = level_m[l];
         uint32_t chunks = (m + (1u << levels.chunk_log) - 1) >> levels.chunk_log;
         uint32_t* run_out = runs[l & 1].ptr;
-        const dim3 grid(levels.tot_len[l], windows);
+        const dim3 grid(levels.tot_len[l], active_windows());
         msm_reduce_level<FC><<<grid, kReduceThreads, kReduceThreads * sizeof(Xyzz<FC>), s>>>(
             in, in_stride, m, levels.chunk_log, l == 0 ? slot_start.ptr : nullptr,
             tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(), levels.tot_len[l], run_out,
@@ -282,7 +316,8 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
       break;
     }
     case kStageWindows: {
-      msm_window_sums<FC><<<windows, kWindowThreads, kWindowThreads * sizeof(Xyzz<FC>), s>>>(tots.ptr, levels,
+      msm_window_sums<FC><<<active_windows(), kWindowThreads, kWindowThreads * sizeof(Xyzz<FC>), s>>>(tots.ptr,
+                                                                                                    levels,
                                                                                             window_sums.ptr);
       check_launch("msm_window_sums");
       break;

@@ -11,6 +11,9 @@ namespace zkg {
 
 uint32_t default_window(size_t n);
 void upload_bases(zkg_ctx* ctx, const uint32_t* xy, size_t words, bool mont256, zkg_buf* out);
+// out (windows * n points) <- the fixed-base table of n resident bases for window size c: row w
+// holds 2^(c w) P_i (windows = ceil(255 / c)); queued on the context stream.
+void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, uint32_t c, zkg_buf* out);
 
 struct MsmPlan {
   enum Stage {
@@ -46,7 +49,14 @@ struct MsmPlan {
   // pass records each digit's rank in its slot, the placing pass runs window by window;
   // msm_rank / msm_place). 1 is the default where it applies (c <= 16).
   int sort_form = 1;
-  bool ranked_sort() const { return sort_form == 1 && c <= 16; }
+  bool ranked_sort() const { return fixed_base || (sort_form == 1 && c <= 16); }
+  // Fixed-base mode: `bases` of run() is a table from fixed_base_table() (windows * n points,
+  // row w = 2^(c w) P_i), every window's digits share one set of 2^(c-1) buckets, and the
+  // result is that set's running sum: no per-window reductions and no combination doublings.
+  // Needs c <= 16 (the ranked sort).
+  bool fixed_base = false;
+  size_t active_slots() const { return fixed_base ? half : slots; }
+  uint32_t active_windows() const { return fixed_base ? 1u : windows; }
   size_t slots = 0, heads_max = 0;
   uint32_t merge_levels = 0, merge_fan_in = 16, scan_tiles_n = 0;
   ReduceLevels levels;
@@ -69,6 +79,7 @@ struct MsmPlan {
   size_t xyzz_words() const;
   size_t affine_words() const;
   void check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const;
+  void set_fixed_base(bool enable);
   // Queues every stage on stream s (no host synchronisation).
   void enqueue(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
   void run(const zkg_buf* bases, const zkg_buf* scalars);

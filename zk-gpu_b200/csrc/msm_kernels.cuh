@@ -182,8 +182,10 @@ __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint
 constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occurs for c <= 16
 constexpr uint32_t kRankOverflow = 0xffffu;
 
+// fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
+// window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
 template <int AGG>
-__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows,
+__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows, int fixed,
                          uint32_t* __restrict__ counts, uint32_t* __restrict__ ranked) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
@@ -191,38 +193,93 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_
   if (live) load_scalar(scalars, i, rc.s);
   const uint32_t half = 1u << (c - 1);
   const unsigned lane = threadIdx.x & 31;
-  for (uint32_t w = 0; w < windows; w++) {
-    bool neg = false;
-    const uint32_t slot = live ? rc.next(w, c, half, &neg) : kNoKey;
-    const unsigned peers = slot_peers<AGG>(slot);
-    const int leader = peers ? __ffs(peers) - 1 : (int)lane;
-    uint32_t base = 0;
-    if (peers && (int)lane == leader) base = atomicAdd(&counts[slot], (uint32_t)__popc(peers));
-    base = __shfl_sync(__activemask(), base, leader);
-    if (!live) continue;
-    uint32_t code = kRankZero;
-    if (peers) {
-      const uint32_t rank = base + __popc(peers & ((1u << lane) - 1));
-      code = (slot - w * half) | (neg ? 0x8000u : 0u) | (min(rank, kRankOverflow) << 16);
+  // Windows four at a time: the four counting atomics (each returns the entry's rank) are in
+  // flight together before any result is used.
+  constexpr int kBatch = 4;
+  for (uint32_t w0 = 0; w0 < windows; w0 += kBatch) {
+    uint32_t slot[kBatch], base[kBatch];
+    unsigned peers[kBatch];
+    bool neg[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const uint32_t w = w0 + k;
+      slot[k] = kNoKey;
+      neg[k] = false;
+      if (w < windows) {  // uniform across the warp
+        if (live) slot[k] = rc.next(w, c, half, &neg[k]);
+        if (fixed && slot[k] != kNoKey) slot[k] -= w * half;
+        peers[k] = slot_peers<AGG>(slot[k]);
+        base[k] = 0;
+        if (peers[k] && (int)lane == __ffs(peers[k]) - 1) base[k] = atomicAdd(&counts[slot[k]], (uint32_t)__popc(peers[k]));
+      }
     }
-    __stcs(ranked + (size_t)w * n + i, code);  // streamed: read once by msm_place
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const uint32_t w = w0 + k;
+      if (w >= windows) break;
+      const int leader = peers[k] ? __ffs(peers[k]) - 1 : (int)lane;
+      const uint32_t b = __shfl_sync(0xffffffffu, base[k], leader);
+      if (!live) continue;
+      uint32_t code = kRankZero;
+      if (peers[k]) {
+        const uint32_t rank = b + __popc(peers[k] & ((1u << lane) - 1));
+        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u) | (min(rank, kRankOverflow) << 16);
+      }
+      __stcs(ranked + (size_t)w * n + i, code);  // streamed: read once by msm_place
+    }
   }
 }
 
 // Grid (ceil(n / 256), windows): blockIdx.y is the window, so blocks run window by window.
-__global__ void msm_place(const uint32_t* __restrict__ ranked, size_t n, uint32_t half,
+// fixed: every window's digits share the buckets, and the entry names point w * n + i of a
+// fixed-base table (2^(c w) P_i at row w).
+__global__ void msm_place(const uint32_t* __restrict__ ranked, size_t n, uint32_t half, int fixed,
                           const uint32_t* __restrict__ slot_start, uint32_t* __restrict__ overflow_cursor,
                           uint32_t* __restrict__ sorted) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const uint32_t w = blockIdx.y;
-  const uint32_t code = __ldcs(ranked + (size_t)w * n + i);
+  const uint32_t code = i < n ? __ldcs(ranked + (size_t)w * n + i) : kRankZero;
   const uint32_t digit = code & 0xffffu;
-  if (digit == kRankZero) return;
-  const uint32_t slot = w * half + (digit & 0x7fffu);
+  const bool valid = digit != kRankZero;
+  const uint32_t slot = (fixed ? 0u : w * half) + (digit & 0x7fffu);
   const uint32_t rank = code >> 16;
-  const uint32_t pos = rank < kRankOverflow ? slot_start[slot] + rank : atomicAdd(&overflow_cursor[slot], 1u);
-  sorted[pos] = (uint32_t)i | ((digit & 0x8000u) ? kNegBit : 0u);
+  // Entries past the rank field (more than 65534 in one slot: skewed scalars) take positions from
+  // the slot's overflow cursor, one atomic per group of lanes with the same slot.
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned over = __ballot_sync(0xffffffffu, valid && rank >= kRankOverflow);
+  uint32_t pos = 0;
+  if (valid && rank >= kRankOverflow) {
+    const unsigned peers = __match_any_sync(over, slot);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(&overflow_cursor[slot], (uint32_t)__popc(peers));
+    pos = __shfl_sync(peers, base, leader) + __popc(peers & ((1u << lane) - 1));
+  } else if (valid) {
+    pos = slot_start[slot] + rank;
+  }
+  if (!valid) return;
+  const uint32_t point = fixed ? (uint32_t)((size_t)w * n + i) : (uint32_t)i;
+  sorted[pos] = point | ((digit & 0x8000u) ? kNegBit : 0u);
+}
+
+// Fixed-base table: row w holds 2^(c w) P_i for every base i (affine, Montgomery form, infinity
+// as zeros), rows 0..windows-1; an MSM over it needs no per-window buckets and no Horner
+// combination. One thread per base: c doublings between rows, one inversion per row.
+template <class F>
+__global__ void msm_fixed_base_table(const uint32_t* __restrict__ bases, size_t n, uint32_t c, uint32_t windows,
+                                     uint32_t* __restrict__ table) {
+  constexpr int AW = PointWords<F>::affine;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Xyzz<F> acc = from_affine(load_affine<F>(bases + i * AW));
+  for (uint32_t w = 0; w < windows; w++) {
+    const Affine<F> a = to_affine(acc);
+    uint32_t* o = table + ((size_t)w * n + i) * AW;
+    store_elem(o, a.x);
+    store_elem(o + AW / 2, a.y);
+    if (w + 1 < windows)
+      for (uint32_t k = 0; k < c; k++) acc = xyzz_double(acc);
+  }
 }
 
 // ------------------------------------------------------------------ scan (3 phases)

@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(kNttThreads, PAIR ? 2 : 3)
           const uint32_t e = b & (size - 1);
           w[k] = (r_lo | j0) != 0
                      ? FqD{{twst[e], twst[size + e], twst[2 * size + e], twst[3 * size + e], twst[4 * size + e]}}
-                     : fqd_one260();  // a product by one in Montgomery form returns the value, below 2r
+                     : frd_one260();  // a product by one in Montgomery form returns the value, below 2r
           x[k] = tile_load_d(tile_d, elems, sa[k]);
           y[k] = tile_load_d(tile_d, elems, sb[k]);
         }
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(kNttThreads, 2)
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
 
-  const FqD one = fqd_one260();
+  const FqD one = frd_one260();
   for (uint32_t st = 0, step = 0; st < s; st += 2, step++) {
     if (st + 2 < s) copy_step((step & 1) ? set0 : set1, st + 2);
     const double* twa = (step & 1) ? set1 : set0;
@@ -602,20 +602,25 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   host::words32(n_inv, n_inv_words);
 
   scratch.alloc(8 * n, "ntt scratch");
-  build_twiddles(w, fwd_tw, seeds[0]);
-  build_twiddles(w_inv, inv_tw, seeds[1]);
-  // Set-up work runs on the set-up stream: done before the plan is used on any stream.
-  check_cuda(cudaStreamSynchronize(ctx->setup), "ntt twiddles");
+  build_seeds(w, seeds[0]);
+  build_seeds(w_inv, seeds[1]);
   set_pass_smem_limits();
-  // Double-precision butterflies by default: on B200 they are 40% faster up to 2^17 elements
-  // (smaller tiles, more blocks), 13% at 2^20 and within 1% from 2^21 to 2^24.
-  set_variant(1);
+  // Double-precision butterflies with staged twiddles by default: on B200 the fastest correct
+  // form, or within 0.002 ms of it, at every size measured (2^24: 5.03 ms against 5.33 for
+  // forms 0 and 1; 2^20: 0.292 against 0.313 / 0.356 ms).
+  set_variant(2);
 }
 
 uint32_t NttPlan::tile_log() const { return variant != 0 ? kTileLogD : kTileLog; }
 
 bool NttPlan::set_variant(int v) {
   if (v < 0 || v > 4) return false;
+  if (v <= 1 && !fwd_tw.ptr) {  // the table of w^j on first use of a form that reads it
+    use(ctx);
+    build_twiddles(seeds[0], fwd_tw);
+    build_twiddles(seeds[1], inv_tw);
+    check_cuda(cudaStreamSynchronize(ctx->setup), "ntt twiddles");
+  }
   if (v == 1 && !fwd_twd.ptr) {  // twiddle limbs on first use of the double-precision form
     const size_t count = (size_t)1 << (log_n - 1);
     use(ctx);
@@ -681,7 +686,9 @@ void NttPlan::build_stage_tables() {
   check_cuda(cudaStreamSynchronize(ctx->setup), "ntt staged twiddles");
 }
 
-void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]) {
+// Seed tables of one direction: lo[j] = w^j (j < 2^lo_bits) and hi[k] = w^(k 2^lo_bits), so
+// that w^j = hi[j >> lo_bits] * lo[j mod 2^lo_bits] for j < n/2 (twiddles.wgsl:13-21).
+void NttPlan::build_seeds(const host::U256& root, DeviceArray (&seed)[2]) {
   const host::Field& f = host::fr();
   const size_t count = (size_t)1 << (log_n - 1);
   const uint32_t lo_bits = (log_n - 1 + 1) / 2;  // ceil((log_n - 1) / 2)
@@ -697,8 +704,14 @@ void NttPlan::build_twiddles(const host::U256& root, DeviceArray& out, DeviceArr
   // From pageable host memory: the call returns once the host vectors have been staged.
   check_cuda(cudaMemcpyAsync(dlo.ptr, lo.data(), lo.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "twiddle copy");
   check_cuda(cudaMemcpyAsync(dhi.ptr, hi.data(), hi.size() * 4, cudaMemcpyHostToDevice, ctx->setup), "twiddle copy");
+}
+
+// The table of w^j, j < n/2, from a direction's seeds (set-up stream).
+void NttPlan::build_twiddles(DeviceArray (&seed)[2], DeviceArray& out) {
+  const size_t count = (size_t)1 << (log_n - 1);
+  const uint32_t lo_bits = (log_n - 1 + 1) / 2;
   out.alloc(8 * count, "ntt twiddles");
-  ntt_twiddles<<<grid_for(count, 256), 256, 0, ctx->setup>>>(dhi.ptr, dlo.ptr, lo_bits, count, out.ptr);
+  ntt_twiddles<<<grid_for(count, 256), 256, 0, ctx->setup>>>(seed[1].ptr, seed[0].ptr, lo_bits, count, out.ptr);
   check_launch("ntt_twiddles");
 }
 

@@ -38,7 +38,7 @@ struct NttPlan {
   // The first switch to form 1 builds its twiddle limbs; form 2 builds its tables for each split
   // (set-up stream, waited for).
   bool set_variant(int variant);
-  int variant = 1;
+  int variant = 2;
   uint32_t tile_log() const;
   // Splits the stages into passes of at most max_stages (6..tile_log()); false if not applicable
   // (transforms of one tile have a single pass).
@@ -59,7 +59,8 @@ struct NttPlan {
   void prepare_shift(const CosetShift& shift);
 
  private:
-  void build_twiddles(const host::U256& root, DeviceArray& out, DeviceArray (&seed)[2]);
+  void build_seeds(const host::U256& root, DeviceArray (&seed)[2]);
+  void build_twiddles(DeviceArray (&seed)[2], DeviceArray& out);
   // Form 2: one table per pass and direction, for the split in `passes`.
   void build_stage_tables();
   std::vector<std::unique_ptr<DeviceArray>> stage_tw[2];

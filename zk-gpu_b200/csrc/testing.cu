@@ -11,41 +11,12 @@
 
 namespace zkg {
 
-// ------------------------------------------------------------------ inversion (Fermat)
-
-// a^(p-2) mod p, square-and-multiply over the exponent bits from the top (a != 0).
-template <class P>
-__device__ Fp<P> fp_inverse(const Fp<P>& a) {
-  const uint32_t e[8] = {P::P0 - 2u, P::P1, P::P2, P::P3, P::P4, P::P5, P::P6, P::P7};  // p0 >= 2
-  Fp<P> acc = Fp<P>::one();
-  for (int bit = 255; bit >= 0; bit--) {
-    acc = acc * acc;
-    if ((e[bit >> 5] >> (bit & 31)) & 1) acc = acc * a;
-  }
-  return acc;
-}
-
-__device__ Fq field_inverse(const Fq& a) { return fp_inverse(a); }
-// 1 / (a + bu) = (a - bu) / (a^2 + b^2)
-__device__ Fq2 field_inverse(const Fq2& x) {
-  Fq inv = fp_inverse(x.a * x.a + x.b * x.b);
-  return Fq2{x.a * inv, neg(x.b * inv)};
-}
-
 __device__ __forceinline__ Fq from_mont(const Fq& a) {
   Fq one_plain = Fq::zero();
   one_plain.w[0] = 1;
   return a * one_plain;
 }
 __device__ __forceinline__ Fq2 from_mont(const Fq2& a) { return Fq2{from_mont(a.a), from_mont(a.b)}; }
-
-// XYZZ -> affine with one inversion: I = 1/(ZZ*ZZZ), 1/ZZ = ZZZ*I, 1/ZZZ = ZZ*I.
-template <class F>
-__device__ Affine<F> to_affine(const Xyzz<F>& p) {
-  if (is_infinity(p)) return Affine<F>{F::zero(), F::zero()};
-  F inv = field_inverse(p.zz * p.zzz);
-  return Affine<F>{p.x * (p.zzz * inv), p.y * (p.zz * inv)};
-}
 
 // ------------------------------------------------------------------ point ops test
 

@@ -71,6 +71,18 @@ class Msm:
         group, 2 none, 3 the first equal neighbour pair's group."""
         check(lib().zkg_msm_set_sort(self._h, mode))
 
+    def set_fixed_base(self, enable: bool = True) -> None:
+        """Runs take a fixed-base table (Msm.fixed_base_table) as their bases: one set of buckets
+        for every window and no combination doublings; the same result as the plain MSM."""
+        check(lib().zkg_msm_set_fixed_base(self._h, int(enable)))
+
+    @staticmethod
+    def fixed_base_table(gpu: Gpu, group: Group, bases: Buffer, n: int, c: int) -> Buffer:
+        """Rows w = 0..ceil(255/c)-1 of 2^(c w) P_i for the n resident bases."""
+        h = vp()
+        check(lib().zkg_msm_fixed_base_table(gpu.handle, int(group), bases.handle, n, c, ctypes.byref(h)))
+        return Buffer(gpu, h.value)
+
     def set_sort_form(self, form: int) -> None:
         """Counting sort: 0 scatter through atomic cursors, 1 ranked placement window by window
         (default for c <= 16)."""
