@@ -169,6 +169,11 @@ int zkg_xyzz_to_affine(const uint32_t *words, uint64_t *x, uint64_t *y);
 /* xyzz_to_affine_g2 (src/msm.rs:356-373): 64 words -> x = (x.a, x.b), y = (y.a, y.b), each
  * coordinate 4 LE u64 (8 u64 per Fq2 value). Returns 1 finite, 0 infinity. */
 int zkg_xyzz_to_affine_g2(const uint32_t *words, uint64_t *x, uint64_t *y);
+/* P + Q for two XYZZ points in this library's memory format (32 words G1, 64 G2; R = 2^256
+ * Montgomery words; infinity has ZZ = 0), on the host: combines the partial results of MSMs
+ * that several GPUs ran over shards of one key (no reference counterpart: the reference runs on
+ * one device). add-2008-s / dbl-2008-s-1 with every special case; out may alias a or b. */
+int zkg_xyzz_add_host(int group, const uint32_t *a, const uint32_t *b, uint32_t *out);
 
 /* ------------------------------------------------------------------ Ntt (src/ntt.rs) */
 

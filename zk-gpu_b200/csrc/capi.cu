@@ -5,6 +5,7 @@
 #include <string>
 
 #include "batch.hpp"
+#include "host_curve.hpp"
 #include "host_field.hpp"
 #include "msm.hpp"
 #include "ntt.hpp"
@@ -469,6 +470,45 @@ int zkg_msm_profile(zkg_msm* msm, const zkg_buf* bases, const zkg_buf* scalars, 
       k++;
     }
     if (count) *count = k;
+  });
+}
+
+namespace {
+host::U256 word_elem(const uint32_t* w) { return host::from_words32(w); }
+void elem_words(const host::U256& e, uint32_t* w) { host::words32(e, w); }
+host::U512 word_elem2(const uint32_t* w) { return host::U512{host::from_words32(w), host::from_words32(w + 8)}; }
+void elem_words2(const host::U512& e, uint32_t* w) {
+  host::words32(e.a, w);
+  host::words32(e.b, w + 8);
+}
+}  // namespace
+
+int zkg_xyzz_add_host(int group, const uint32_t* a, const uint32_t* b, uint32_t* out) {
+  return guard([&] {
+    need(a, "a");
+    need(b, "b");
+    need(out, "out");
+    if (group == ZKG_G1) {
+      using P = host::XyzzH<host::U256>;
+      const P pa{word_elem(a), word_elem(a + 8), word_elem(a + 16), word_elem(a + 24)};
+      const P pb{word_elem(b), word_elem(b + 8), word_elem(b + 16), word_elem(b + 24)};
+      const P r = host::xyzz_add_h(pa, pb);
+      elem_words(r.x, out);
+      elem_words(r.y, out + 8);
+      elem_words(r.zz, out + 16);
+      elem_words(r.zzz, out + 24);
+    } else if (group == ZKG_G2) {
+      using P = host::XyzzH<host::U512>;
+      const P pa{word_elem2(a), word_elem2(a + 16), word_elem2(a + 32), word_elem2(a + 48)};
+      const P pb{word_elem2(b), word_elem2(b + 16), word_elem2(b + 32), word_elem2(b + 48)};
+      const P r = host::xyzz_add_h(pa, pb);
+      elem_words2(r.x, out);
+      elem_words2(r.y, out + 16);
+      elem_words2(r.zz, out + 32);
+      elem_words2(r.zzz, out + 48);
+    } else {
+      fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
+    }
   });
 }
 

@@ -73,6 +73,7 @@ SIGNATURES = {
     "zkg_msm_fixed_base_table": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.c_uint32,
                                                 ctypes.POINTER(vp)]),
     "zkg_msm_set_fixed_base": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_xyzz_add_host": (ctypes.c_int, [ctypes.c_int, u32p, u32p, u32p]),
     "zkg_quotient": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32, u32p]),
     "zkg_zkey_parse": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "zkg_zkey_free": (None, [vp]),
