@@ -210,8 +210,13 @@ __global__ void __launch_bounds__(kNttThreads, 3)
       const uint32_t idx = ((r_lo << lm) + j0) << t;
       const FqD x = tile_load_d(tile_d, elems, slot_a);
       const FqD y = tile_load_d(tile_d, elems, slot_b);
-      tile_store_d(tile_d, elems, slot_a, fqd_reduce<FrLimbs>(fqd_add(x, y), kr));
-      const FqD d = fqd_sub<2, FrLimbs>(x, y);  // (0, 4r)
+      // Values enter even stages below 2r and odd stages below 4r: an even stage leaves its sums
+      // unreduced (below 4r) unless it is the pass's last; an odd stage reduces them (from below
+      // 8r). Differences get 4r added in odd stages, so products see inputs below 8r.
+      const bool odd = st & 1;
+      const FqD sum = fqd_add(x, y);
+      tile_store_d(tile_d, elems, slot_a, (odd || st + 1 == s) ? fqd_reduce<FrLimbs>(sum, kr) : sum);
+      const FqD d = odd ? fqd_sub<4, FrLimbs>(x, y) : fqd_sub<2, FrLimbs>(x, y);  // (0, 8r)
       FqD out;
       if (idx != 0) {
         const double* w = tw + 5 * (size_t)idx;
@@ -441,8 +446,13 @@ __global__ void __launch_bounds__(kNttThreads, PAIR ? 2 : 3)
       const uint32_t j0 = c & ((1u << lm) - 1);
       const FqD x = tile_load_d(tile_d, elems, slot_a);
       const FqD y = tile_load_d(tile_d, elems, slot_b);
-      tile_store_d(tile_d, elems, slot_a, fqd_reduce<FrLimbs>(fqd_add(x, y), kr));
-      const FqD d = fqd_sub<2, FrLimbs>(x, y);  // (0, 4r)
+      // Values enter even stages below 2r and odd stages below 4r: an even stage leaves its sums
+      // unreduced (below 4r) unless it is the pass's last; an odd stage reduces them (from below
+      // 8r). Differences get 4r added in odd stages, so products see inputs below 8r.
+      const bool odd = st & 1;
+      const FqD sum = fqd_add(x, y);
+      tile_store_d(tile_d, elems, slot_a, (odd || st + 1 == s) ? fqd_reduce<FrLimbs>(sum, kr) : sum);
+      const FqD d = odd ? fqd_sub<4, FrLimbs>(x, y) : fqd_sub<2, FrLimbs>(x, y);  // (0, 8r)
       FqD out;
       if ((r_lo | j0) != 0) {
         const uint32_t e = b & (size - 1);
