@@ -133,8 +133,9 @@ int zkg_msm_set_variant(zkg_msm *msm, int variant);
 int zkg_msm_set_sort(zkg_msm *msm, int mode);
 /* Counting-sort form (no reference counterpart): 0 = one pass scatters every (window, point)
  * entry through an atomic cursor per slot; 1 = the counting pass also records each entry's
- * rank within its slot, and the placing pass writes the entries window by window, so the
- * stores of one window meet in L2 (default; applies for c <= 16, larger c use 0). */
+ * rank within its slot (and its digit), and the placing pass writes the entries window by
+ * window, so the stores of one window meet in L2 (default; applies for c <= 16, larger c use 0;
+ * 6 more bytes of plan memory per (window, point) entry). */
 int zkg_msm_set_sort_form(zkg_msm *msm, int form);
 /* Fixed-base MSM over a resident key (no reference counterpart: the reference combines its
  * windows by Horner, msm_combine.wgsl:13-22, on every run). zkg_msm_fixed_base_table builds, once

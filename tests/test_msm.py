@@ -406,9 +406,8 @@ def test_sort_aggregation_modes_agree(gpu, mode, form):
 
 @pytest.mark.parametrize("form", [0, 1])
 def test_slots_beyond_the_rank_field(gpu, form):
-    """More than 65534 entries in one slot (every scalar 1, or r - 1: all points in one bucket of
-    window 0): the ranked sort places the entries past the 16-bit rank through its overflow
-    cursor."""
+    """More than 2^16 entries in one slot (every scalar 1, or r - 1: all points in one bucket of
+    window 0), in both sort forms: ranks past 16 bits place correctly."""
     n = (1 << 17) + 3
     bases = random_points("G1", 970, n)
     for s in (fr_words([1] * n), fr_words([R - 1] * (n - 5) + [2, 3, 0, 7, R - 2])):

@@ -85,7 +85,10 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (scan_tiles_n > (uint32_t)kScanTile) fail(ZKG_EINVAL, "too many bucket slots");
   tile_sums.alloc(scan_tiles_n, "msm scan tiles");
   sorted.alloc(max_entries, "msm sorted");
-  if (c <= 16) ranked.alloc(max_entries, "msm ranked digits");
+  if (c <= 16) {
+    ranks.alloc(max_entries, "msm ranks");
+    digits.alloc((max_entries + 1) / 2, "msm ranked digits");  // 16 bits per entry
+  }
   buckets.alloc(slots * xw, "msm buckets");
 
   heads_max = (max_entries + seg_len - 1) / seg_len;
@@ -187,16 +190,16 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       if (ranked_sort()) {
         if (sort_agg == 0)
           msm_rank<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                ranked.ptr);
+                                                                digits.as<uint16_t>(), ranks.ptr);
         else if (sort_agg == 1)
           msm_rank<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                ranked.ptr);
+                                                                digits.as<uint16_t>(), ranks.ptr);
         else if (sort_agg == 2)
           msm_rank<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                ranked.ptr);
+                                                                digits.as<uint16_t>(), ranks.ptr);
         else
           msm_rank<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                ranked.ptr);
+                                                                digits.as<uint16_t>(), ranks.ptr);
         check_launch("msm_rank");
       } else if (sort_agg == 1)
         msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
@@ -217,14 +220,15 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       scan_tiles<<<1, kScanBlock, 0, s>>>(tile_sums.ptr, tiles, slot_start.ptr + ns);
       check_launch("scan_tiles");
       scan_apply<<<tiles, kScanBlock, 0, s>>>(counts.ptr, ns, tile_sums.ptr, slot_start.ptr, cursor.ptr,
-                                                     ranked_sort() ? kRankOverflow : 0u);
+                                                     0u);
       check_launch("scan_apply");
       break;
     }
     case kStageScatter:
       if (ranked_sort()) {
         const dim3 grid((unsigned)grid_for(n, b256), windows);
-        msm_place<<<grid, b256, 0, s>>>(ranked.ptr, n, half, fixed_base, slot_start.ptr, cursor.ptr, sorted.ptr);
+        msm_place<<<grid, b256, 0, s>>>(digits.as<uint16_t>(), ranks.ptr, n, half, fixed_base, slot_start.ptr,
+                                        sorted.ptr);
         check_launch("msm_place");
         break;
       }

@@ -63,7 +63,7 @@ struct MsmPlan {
   std::vector<uint32_t> level_m;
 
   DeviceArray counts, slot_start, cursor, tile_sums, sorted, buckets;
-  DeviceArray ranked;  // the ranked sort's digit and rank per (window, point), window-major
+  DeviceArray ranks, digits;  // the ranked sort's rank (32 bits) and digit (16 bits) per (window, point), window-major
   DeviceArray heads[2], head_keys[2];
   DeviceArray tots, runs[2], window_sums, result;
   zkg_buf result_handle;

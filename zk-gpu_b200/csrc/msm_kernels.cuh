@@ -170,23 +170,22 @@ __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint
 //
 // The same sort in two passes without scattered stores over the whole sorted array:
 //   msm_rank  recodes each scalar once; the warp-aggregated atomic that counts a digit also
-//             returns its rank within its slot; digit and rank go to a window-major array
-//             (entry w * n + i: bits 0..15 the digit, bucket | sign << 15, 0x7fff for a zero
-//             digit; bits 16..31 the rank, 0xffff when it does not fit) with coalesced stores.
+//             returns its rank within its slot; the digit (bucket | sign << 15, kRankZero for a
+//             zero digit; 16 bits) and the rank (32 bits) go to window-major arrays (entry
+//             w * n + i) with coalesced streaming stores.
 //   msm_place after the scan, walks the entries window by window: sorted[slot_start + rank] =
 //             point index | sign. A window's slots span ~4n bytes of the sorted array, so the
-//             4-byte stores of the blocks in flight meet in L2 and reach HBM as whole sectors
-//             (the scalar-major scatter touches all windows' ranges at once: 1 GiB at 2^24).
-// Ranks of 0xffff and above (a slot with more than 65534 entries: skewed scalars) are placed
-// through an atomic cursor that starts at slot_start + 0xffff. For c <= 16 (15-bit buckets).
+//             4-byte stores of the blocks in flight meet in L2 (the scalar-major scatter touches
+//             all windows' ranges at once: 1 GiB at 2^24), and no pass needs a second atomic.
+// For c <= 16 (15-bit buckets).
 constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occurs for c <= 16
-constexpr uint32_t kRankOverflow = 0xffffu;
 
 // fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
 // window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
 template <int AGG>
 __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows, int fixed,
-                         uint32_t* __restrict__ counts, uint32_t* __restrict__ ranked) {
+                         uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
+                         uint32_t* __restrict__ ranks) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
   Recoder rc;
@@ -221,11 +220,12 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_
       const uint32_t b = __shfl_sync(0xffffffffu, base[k], leader);
       if (!live) continue;
       uint32_t code = kRankZero;
+      const size_t e = (size_t)w * n + i;
       if (peers[k]) {
-        const uint32_t rank = b + __popc(peers[k] & ((1u << lane) - 1));
-        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u) | (min(rank, kRankOverflow) << 16);
+        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);
+        __stcs(ranks + e, b + __popc(peers[k] & ((1u << lane) - 1)));  // streamed: read once by msm_place
       }
-      __stcs(ranked + (size_t)w * n + i, code);  // streamed: read once by msm_place
+      __stcs(digits + e, (unsigned short)code);
     }
   }
 }
@@ -233,33 +233,18 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_
 // Grid (ceil(n / 256), windows): blockIdx.y is the window, so blocks run window by window.
 // fixed: every window's digits share the buckets, and the entry names point w * n + i of a
 // fixed-base table (2^(c w) P_i at row w).
-__global__ void msm_place(const uint32_t* __restrict__ ranked, size_t n, uint32_t half, int fixed,
-                          const uint32_t* __restrict__ slot_start, uint32_t* __restrict__ overflow_cursor,
+__global__ void msm_place(const uint16_t* __restrict__ digits, const uint32_t* __restrict__ ranks, size_t n,
+                          uint32_t half, int fixed, const uint32_t* __restrict__ slot_start,
                           uint32_t* __restrict__ sorted) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
   const uint32_t w = blockIdx.y;
-  const uint32_t code = i < n ? __ldcs(ranked + (size_t)w * n + i) : kRankZero;
-  const uint32_t digit = code & 0xffffu;
-  const bool valid = digit != kRankZero;
+  const size_t e = (size_t)w * n + i;
+  const uint32_t digit = __ldcs(digits + e);
+  if (digit == kRankZero) return;
   const uint32_t slot = (fixed ? 0u : w * half) + (digit & 0x7fffu);
-  const uint32_t rank = code >> 16;
-  // Entries past the rank field (more than 65534 in one slot: skewed scalars) take positions from
-  // the slot's overflow cursor, one atomic per group of lanes with the same slot.
-  const unsigned lane = threadIdx.x & 31;
-  const unsigned over = __ballot_sync(0xffffffffu, valid && rank >= kRankOverflow);
-  uint32_t pos = 0;
-  if (valid && rank >= kRankOverflow) {
-    const unsigned peers = __match_any_sync(over, slot);
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if ((int)lane == leader) base = atomicAdd(&overflow_cursor[slot], (uint32_t)__popc(peers));
-    pos = __shfl_sync(peers, base, leader) + __popc(peers & ((1u << lane) - 1));
-  } else if (valid) {
-    pos = slot_start[slot] + rank;
-  }
-  if (!valid) return;
-  const uint32_t point = fixed ? (uint32_t)((size_t)w * n + i) : (uint32_t)i;
-  sorted[pos] = point | ((digit & 0x8000u) ? kNegBit : 0u);
+  const uint32_t point = fixed ? (uint32_t)e : (uint32_t)i;
+  sorted[slot_start[slot] + __ldcs(ranks + e)] = point | ((digit & 0x8000u) ? kNegBit : 0u);
 }
 
 // Fixed-base table: row w holds 2^(c w) P_i for every base i (affine, Montgomery form, infinity

@@ -117,8 +117,8 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
     const size_t B = (size_t)1 << (c - 1), S = (size_t)W * B;
     const size_t entries = (size_t)W * m, L = 8;  // worst case of the automatic segment length
     const size_t heads = entries / L + 1;
-    // counts, slot starts, cursors; sorted and ranked entries; buckets; heads; running sums
-    return 4 * (3 * S + 2 * entries + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
+    // counts, slot starts, cursors; sorted entries, ranks and digits; buckets; heads; running sums
+    return 4 * (3 * S + entries * 5 / 2 + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
   };
   // scratch, twiddle words (both directions), staged twiddle tables (both directions: 40 bytes
   // per element for the first pass, at most as much again for the later passes' small tables
