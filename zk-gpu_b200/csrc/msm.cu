@@ -36,6 +36,14 @@ static void set_acc_smem_limits() {
              "accumulation smem attribute");
 }
 
+// The last reduction level's block holds one XYZZ point per thread in shared memory: 64 KiB for
+// G2 (256 threads x 256 bytes), above the default limit.
+static void set_scan_smem_limits() {
+  const int bytes = (int)(kScanThreads * sizeof(Xyzz<Fq2CP>));
+  check_cuda(cudaFuncSetAttribute(msm_reduce_scan<Fq2CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+             "reduction smem attribute");
+}
+
 uint32_t default_window(size_t n) {
   // clamp(log2(max(n,1)) - 5, 11, 16) (src/msm.rs:78-80)
   size_t v = n < 1 ? 1 : n;
@@ -77,7 +85,10 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
 
   use(ctx);
-  if (group == ZKG_G2) set_acc_smem_limits();
+  if (group == ZKG_G2) {
+    set_acc_smem_limits();
+    set_scan_smem_limits();
+  }
   counts.alloc(slots, "msm counts");
   slot_start.alloc(slots + 1, "msm slot_start");
   cursor.alloc(slots, "msm cursor");
@@ -119,6 +130,14 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   std::vector<uint32_t> ms;
   while (m > 0) {
     if (levels.count >= (uint32_t)kMaxReduceLevels) fail(ZKG_EINVAL, "too many reduction levels");
+    if (m <= kScanLevelMax) {  // the last level: one block per window sums it whole (msm_reduce_scan)
+      ms.push_back(m);
+      levels.tot_len[levels.count] = 1;
+      levels.tot_offset[levels.count] = (uint32_t)tot_points;
+      tot_points += windows;
+      levels.count++;
+      break;
+    }
     uint32_t chunks = (m + chunk - 1) / chunk;
     uint32_t blocks = (chunks + kReduceThreads - 1) / kReduceThreads;  // one tot point per block
     ms.push_back(m);
@@ -306,6 +325,13 @@ void MsmPlan::tail_stage(int which, cudaStream_t s) {
       uint32_t in_stride = half;
       for (uint32_t l = 0; l < levels.count; l++) {
         uint32_t m = level_m[l];
+        if (m <= kScanLevelMax) {  // the last level
+          msm_reduce_scan<FC><<<active_windows(), kScanThreads, kScanThreads * sizeof(Xyzz<FC>), s>>>(
+              in, in_stride, m, l == 0 ? slot_start.ptr : nullptr, tots.ptr + (size_t)levels.tot_offset[l] * xyzz_words(),
+              levels.tot_len[l]);
+          check_launch("msm_reduce_scan");
+          break;
+        }
         uint32_t chunks = (m + (1u << levels.chunk_log) - 1) >> levels.chunk_log;
         uint32_t* run_out = runs[l & 1].ptr;
         const dim3 grid(levels.tot_len[l], active_windows());

@@ -15,6 +15,10 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 constexpr int kWindowThreads = 128;
 constexpr int kReduceThreads = 128;  // one running-sum block covers this many chunks of one window
 constexpr int kMaxReduceLevels = 16;
+// The last running-sum level takes at most this many values per window and is summed by one
+// block (msm_reduce_scan) instead of further levels.
+constexpr uint32_t kScanLevelMax = 1024;
+constexpr int kScanThreads = 256;
 
 struct ReduceLevels {
   uint32_t count;                         // levels

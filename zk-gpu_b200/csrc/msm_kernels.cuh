@@ -563,6 +563,49 @@ __global__ void __launch_bounds__(kReduceThreads) msm_reduce_level(const uint32_
 }
 
 
+// The last level: S = sum_b (b + 1) A_b over m <= kScanLevelMax values per window in one block
+// (grid: windows). Thread t owns K = m_pad / 256 consecutive values (K a power of two, at most 4)
+// and forms ls_t = sum_j (j + 1) A_{Kt+j} and lt_t = sum_j A_{Kt+j}; then S = sum_t ls_t +
+// K sum_{t >= 1} suf_t with suf_t = sum_{u >= t} lt_u, a suffix scan over the threads (Hillis-
+// Steele in shared memory) followed by one block sum: about 2K + 2 log2(256) + 2 dependent
+// additions, where further chunked levels would each add a chain and a block sum.
+template <class F>
+__global__ void __launch_bounds__(kScanThreads) msm_reduce_scan(const uint32_t* __restrict__ in, uint32_t in_stride,
+                                                                uint32_t m, const uint32_t* __restrict__ slot_start,
+                                                                uint32_t* __restrict__ tot_out, uint32_t tot_stride) {
+  constexpr int XW = PointWords<F>::xyzz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Xyzz<F>* sh = reinterpret_cast<Xyzz<F>*>(smem_raw);
+  const uint32_t w = blockIdx.x, t = threadIdx.x;
+  uint32_t k = 1;
+  while (k * kScanThreads < m) k <<= 1;
+  Xyzz<F> run = xyzz_infinity<F>(), ls = xyzz_infinity<F>();
+  for (uint32_t j = k; j-- > 0;) {
+    const uint32_t b = t * k + j;
+    if (b >= m) continue;
+    const size_t slot = (size_t)w * in_stride + b;
+    const bool empty = slot_start && __ldg(&slot_start[slot]) == __ldg(&slot_start[slot + 1]);
+    if (!empty) run = xyzz_add(run, load_xyzz<F>(in + slot * XW));
+    ls = xyzz_add(ls, run);
+  }
+  // suffix sums of the threads' totals
+  Xyzz<F> suf = run;
+  sh[t] = suf;
+  __syncthreads();
+  for (uint32_t d = 1; d < kScanThreads; d <<= 1) {
+    const Xyzz<F> other = t + d < kScanThreads ? sh[t + d] : xyzz_infinity<F>();
+    __syncthreads();
+    suf = xyzz_add(suf, other);
+    sh[t] = suf;
+    __syncthreads();
+  }
+  Xyzz<F> next = t + 1 < kScanThreads ? sh[t + 1] : xyzz_infinity<F>();
+  __syncthreads();
+  for (uint32_t kk = k; kk > 1; kk >>= 1) next = xyzz_double(next);  // K suf_{t+1}
+  const Xyzz<F> total = block_sum(xyzz_add(ls, next), sh);
+  if (t == 0) store_xyzz(tot_out + (size_t)w * tot_stride * XW, total);
+}
+
 // One block per window: S_w = sum over levels l of C^l * sum_k tot_l[k] (C = 2^chunk_log),
 // folded from the top level down (chunk_log doublings per level) by warp 0 with lane-parallel
 // products.
