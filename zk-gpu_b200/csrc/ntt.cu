@@ -615,10 +615,11 @@ NttPlan::NttPlan(zkg_ctx* c, uint32_t log_n_) : ctx(c), log_n(log_n_) {
   build_seeds(w, seeds[0]);
   build_seeds(w_inv, seeds[1]);
   set_pass_smem_limits();
-  // Double-precision butterflies with staged twiddles by default: on B200 the fastest correct
-  // form, or within 0.002 ms of it, at every size measured (2^24: 5.03 ms against 5.33 for
-  // forms 0 and 1; 2^20: 0.292 against 0.313 / 0.356 ms).
-  set_variant(2);
+  // Double-precision butterflies with staged twiddles by default, two per thread step up to 2^17
+  // elements: measured on B200 (ms per transform) 2^16: form 3 0.048, form 2 0.050, form 1
+  // 0.054, form 0 0.089; 2^20: form 2 0.292, form 3 0.302, form 1 0.313; 2^24: form 2 5.00,
+  // form 3 5.30, forms 0 and 1 5.33.
+  set_variant(log_n <= 17 ? 3 : 2);
 }
 
 uint32_t NttPlan::tile_log() const { return variant != 0 ? kTileLogD : kTileLog; }
