@@ -40,12 +40,13 @@ IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m
 FP64_PER_MULMOD = 170  # double-precision instructions per Fq product in limb form, field_f64.cuh
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
 # ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured on a G1 MSM of
-# 2^22 points (7.05 GB) and scaled by the entry count to 2^24 (x4); ntt_pass / ntt_pass_f64:
+# 2^22 points (7.05 GB) and scaled by the entry count to 2^24 (x4); NTT forms 0, 1 and 2: the
 # first pass captured on the 2^24 transform.
 NCU_TRAFFIC = {
     "msm_accumulate_2^24": 28.2e9,
     "ntt_form0_2^24": 1.96e9,
     "ntt_form1_2^24": 2.18e9,
+    "ntt_form2_2^24": 1.71e9,
 }
 # The pass kernel of each NTT form.
 NTT_KERNEL = {0: "ntt_pass", 1: "ntt_pass_f64", 2: "ntt_pass_f64s", 3: "ntt_pass_f64s", 4: "ntt_pass_f64r4"}
