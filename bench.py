@@ -543,6 +543,35 @@ def run_configs(gpu, bases, stream, n_max, cpu_too=True) -> dict:
         plain.close()
         tuned.close()
     out["g1_msm_c0_c2"] = c2
+    # fixed-base tables over the resident key (one set of buckets for every window, no
+    # combination): the table build once, then one call, uniform scalars
+    fb = {"method": "zkg_msm_fixed_base_table once (wall time, device synchronised), then one call (device "
+                    "time, best of 3); default_window; the same scalars as the default_window rows above"}
+    for lg in (16, 20):
+        n = 1 << lg
+        if n > n_max:
+            continue
+        c = Msm.default_window(n)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        table = Msm.fixed_base_table(gpu, Group.G1, bases, n, c)
+        gpu.wait()
+        build_ms = (time.perf_counter() - t0) * 1e3
+        msm = Msm(gpu, n, c)
+        msm.set_fixed_base(True)
+        sh = scalar_distribution(n, "uniform", 1400 + lg)
+        sk = gpu.buffer(sh)
+        row = {"ms": device_ms(lambda: msm.run(gpu, table, sk)), "table_build_ms": round(build_ms, 1),
+               "table_bytes": int(table.words() * 4)}
+        if cpu_too:
+            got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, table, sk), 32)))
+            row["bit_exact"] = bool(np.array_equal(got, cpu.msm("G1", host_bases[: 16 * n], sh, mont256=True,
+                                                                 nthreads=threads)))
+        fb[f"2^{lg}"] = row
+        msm.close()
+        sk.free()
+        table.free()
+    out["g1_msm_fixed_base"] = fb
     g2 = {}
     n2 = 1 << 22
     b2 = generator_multiples(gpu, Group.G2, uniform_scalars(n2, 500), mont256=True)
