@@ -148,6 +148,17 @@ int zkg_msm_set_sort_form(zkg_msm *msm, int form);
  * table holds windows times the key's memory. */
 int zkg_msm_fixed_base_table(zkg_ctx *ctx, int group, const zkg_buf *bases, size_t n, uint32_t c, zkg_buf **out);
 int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
+/* GLV splitting for G1 (no reference counterpart; the reference names GLV as a next step,
+ * README.md:223-224): with enable = 1 every scalar k is split as k1 + k2 lambda (mod r), |k1|,
+ * |k2| < 2^127, and a run sums k1_i P_i + k2_i phi(P_i) with phi(x, y) = (beta x, y): 2n points
+ * (the plan makes phi(P_i) from `bases` on every run, 128 more bytes of plan memory per point)
+ * with ceil(128 / c) windows instead of ceil(255 / c), so the same number of bucket additions
+ * and half the bucket reductions and combination doublings. The result is the same point as the
+ * plain MSM (scalars are taken mod r). Needs G1, c <= 16, no fixed-base table and n < 2^30;
+ * otherwise ZKG_EINVAL. Re-sizes the plan's scratch (synchronises with queued work).
+ * zkg_msm_windows reports the plan's window count and whether GLV is on. */
+int zkg_msm_set_glv(zkg_msm *msm, int enable);
+int zkg_msm_windows(const zkg_msm *msm, uint32_t *windows, int *glv);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,
@@ -407,6 +418,11 @@ int zkg_bench_integer_pipe(zkg_ctx *ctx, int variant, double *ops_per_second);
  * of `count` affine pairs (P, Q) in Montgomery form (32 words G1 / 64 words G2 per pair), writes
  * three XYZZ points: P + Q (mixed add), 2P (double), (P + Q) + 2P (full add). */
 int zkg_test_point_ops(zkg_ctx *ctx, int group, const uint32_t *pairs, size_t count, uint32_t *out);
+
+/* The device's GLV split (zkg_msm_set_glv) of `count` scalars in host memory (8 words each):
+ * out[10 i ..] = |k1| (4 words), |k2| (4 words), sign of k1, sign of k2 (1 = negative), with k =
+ * k1 + k2 lambda (mod r), lambda = 0x30644e72e131a029048b6e193fd84104cc37a73fec2bc5e9b8ca0b2d36636f23. */
+int zkg_test_glv_split(zkg_ctx *ctx, const uint32_t *scalars, size_t count, uint32_t *out);
 
 /* Fixed-base batch multiplication: out[i] = [k_i] G for the standard generator of `group`
  * (G1 = (1, 2)), as affine points in plain (mont256 = 0) or Montgomery-2^256 (mont256 = 1)

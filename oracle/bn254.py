@@ -17,6 +17,9 @@ It restates, with Python integers, the mathematics of the reference's path:
                                                      src/shaders/msm_combine.wgsl
 * DIF NTT, natural order in/out, inverse with 1/n . src/ntt.rs:26-68, src/shaders/ntt.wgsl:50-73
 * xyzz_to_affine / xyzz_to_affine_g2 .............. src/msm.rs:345-387
+* GLV split of a G1 scalar (the B200 build's G1 GLV mode; the reference names GLV as its next
+  step, README.md:223-224, and has no code for it) ... Gallant, Lambert, Vanstone, CRYPTO
+  2001: constants derived below from Q and R alone
 
 Pinned against the reference's golden vectors (tests/golden/{ntt,msm}.json, produced by
 ffjavascript 0.3.1, an implementation independent of arkworks) by tests/test_oracle.py.
@@ -401,3 +404,61 @@ def self_check() -> None:
 
 def g2_generator():
     return (Fq2(*G2_GEN[0]), Fq2(*G2_GEN[1]))
+
+
+# ---------------------------------------------------------------- GLV split (G1)
+
+def _cube_root(m: int) -> int:
+    """The first g^((m-1)/3) != 1 over g = 2, 3, ...: a primitive cube root of unity mod m."""
+    g = 2
+    while pow(g, (m - 1) // 3, m) == 1:
+        g += 1
+    return pow(g, (m - 1) // 3, m)
+
+
+def _glv_basis(lam: int):
+    """Short vectors (a1, b1), (a2, b2) with a + b lam = 0 (mod R), by the extended Euclidean
+    algorithm on (R, lam) (Guide to Elliptic Curve Cryptography, algorithm 3.74)."""
+    import math
+    rows = [(R, 0), (lam, 1)]
+    while rows[-1][0] != 0:
+        (r0, t0), (r1, t1) = rows[-2], rows[-1]
+        q = r0 // r1
+        rows.append((r0 - q * r1, t0 - q * t1))
+    root = math.isqrt(R)
+    ell = max(i for i, (r, _) in enumerate(rows) if r >= root)
+    a1, b1 = rows[ell + 1][0], -rows[ell + 1][1]
+    cand = [(rows[ell][0], -rows[ell][1]), (rows[ell + 2][0], -rows[ell + 2][1])]
+    a2, b2 = min(cand, key=lambda v: v[0] * v[0] + v[1] * v[1])
+    return a1, b1, a2, b2
+
+
+_GLV = None
+
+
+def glv_constants() -> dict:
+    """beta (Fq), lambda (Fr) with (beta x, y) = lambda (x, y) on G1, the lattice basis and the
+    fixed-point rounding constants g1 = round(2^256 b2 / r), g2 = round(2^256 (-b1) / r)."""
+    global _GLV
+    if _GLV is None:
+        beta, lam0 = _cube_root(Q), _cube_root(R)
+        probe = scalar_mul(_FqOps, G1_GEN, 0x1234567)
+        lam = next(l for l in (lam0, lam0 * lam0 % R)
+                   if scalar_mul(_FqOps, probe, l) == (beta * probe[0] % Q, probe[1]))
+        a1, b1, a2, b2 = _glv_basis(lam)
+        assert a1 * b2 - a2 * b1 == R
+        rnd = lambda num: (2 * num * (1 << 256) + R) // (2 * R)
+        _GLV = {"beta": beta, "lambda": lam, "a1": a1, "b1": b1, "a2": a2, "b2": b2,
+                "g1": rnd(b2), "g2": rnd(-b1)}
+    return _GLV
+
+
+def glv_split(k: int) -> tuple[int, int]:
+    """k (any 256-bit value, taken mod r) -> (k1, k2), signed, k = k1 + k2 lambda (mod r):
+    c1 = floor((k g1 + 2^255) / 2^256), c2 = floor((k g2 + 2^255) / 2^256), k1 = k - c1 a1 -
+    c2 a2, k2 = -c1 b1 - c2 b2."""
+    g = glv_constants()
+    k %= R
+    c1 = (k * g["g1"] + (1 << 255)) >> 256
+    c2 = (k * g["g2"] + (1 << 255)) >> 256
+    return k - c1 * g["a1"] - c2 * g["a2"], -c1 * g["b1"] - c2 * g["b2"]

@@ -43,10 +43,10 @@ def msm_ref(group: str, bases: np.ndarray, scalars: np.ndarray, mont256: bool = 
 
 
 def gpu_msm(gpu, bases: np.ndarray, scalars: np.ndarray, plan=None, group: Group = Group.G1,
-            variant=None) -> np.ndarray:
+            variant=None, glv=None) -> np.ndarray:
     """Upload plain bases and scalars, run one MSM and return the affine result words
     (zeros = infinity). plan = None uses the defaults; (c, item_points) overrides them;
-    variant selects the accumulation kernel's form."""
+    variant selects the accumulation kernel's form; glv switches the G1 GLV split on or off."""
     n = scalars.size // 8
     base_buf = Msm.upload_bases(gpu, bases)
     scalar_buf = gpu.buffer(scalars)
@@ -56,6 +56,8 @@ def gpu_msm(gpu, bases: np.ndarray, scalars: np.ndarray, plan=None, group: Group
         msm = Msm.for_group(gpu, group, n, plan[0], plan[1])
     if variant is not None:
         msm.set_variant(variant)
+    if glv is not None:
+        msm.set_glv(glv)
     out = msm.run(gpu, base_buf, scalar_buf)
     words = gpu.read(out, group.xyzz_words())
     if group == Group.G1:

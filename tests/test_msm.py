@@ -291,7 +291,7 @@ def test_fuzz(gpu):
 
 # ---------------------------------------------------------------- full sizes
 
-def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False):
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False, glv=None):
     """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
     uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G. tuned: the plan
     (window, points per thread, form) comes from the autotuner on these inputs."""
@@ -313,10 +313,12 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant
         msm = Msm(gpu, n, c)
         if variant is not None:
             msm.set_variant(variant)
+        if glv is not None:
+            msm.set_glv(glv)
     got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, scalar_buf), 32)))
     gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
     want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
-    assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}, variant = {variant}) wrong"
+    assert np.array_equal(got, want), f"G1 MSM 2^{log_n} ({kind}, c = {c}, variant = {variant}, glv = {glv}) wrong"
     # spot check the device-built bases against the CPU
     for i in (0, 1, n - 1):
         assert np.array_equal(plain[16 * i: 16 * i + 16], cpu.generator_multiples("G1", k[8 * i: 8 * i + 8]))

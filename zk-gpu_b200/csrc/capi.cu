@@ -429,6 +429,30 @@ int zkg_msm_set_fixed_base(zkg_msm* msm, int enable) {
   });
 }
 
+int zkg_msm_set_glv(zkg_msm* msm, int enable) {
+  return guard([&] {
+    need(msm, "msm");
+    msm->plan.set_glv(enable != 0);
+  });
+}
+
+int zkg_msm_windows(const zkg_msm* msm, uint32_t* windows, int* glv) {
+  return guard([&] {
+    need(msm, "msm");
+    if (windows) *windows = msm->plan.windows;
+    if (glv) *glv = msm->plan.glv ? 1 : 0;
+  });
+}
+
+int zkg_test_glv_split(zkg_ctx* ctx, const uint32_t* scalars, size_t count, uint32_t* out) {
+  return guard([&] {
+    need(ctx, "ctx");
+    need(scalars, "scalars");
+    need(out, "out");
+    if (count) glv_split(ctx, scalars, count, out);
+  });
+}
+
 int zkg_msm_params(const zkg_msm* msm, uint32_t* c, uint32_t* item_points, int* variant) {
   return guard([&] {
     need(msm, "msm");

@@ -73,22 +73,36 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (c < 9 || c > 20) fail(ZKG_EINVAL, "window size c must be in 9..=20, got " + std::to_string(c));
   if (group != ZKG_G1 && group != ZKG_G2) fail(ZKG_EINVAL, "group must be ZKG_G1 or ZKG_G2");
   if (n >= (size_t)kNegBit) fail(ZKG_EINVAL, "an MSM holds fewer than 2^31 points");
-  windows = (255 + c - 1) / c;
-  half = 1u << (c - 1);
-  slots = (size_t)windows * half;
-  seg_len = item_points ? item_points : auto_seg_len(n, windows);
-  const size_t xw = xyzz_words();
-  const size_t max_entries = (size_t)windows * n;
+  item_points_req = item_points;
+  const size_t max_entries = (size_t)((255 + c - 1) / c) * n;
   // G1: FP64 limbs, two products per call below 2^26 (window, point) entries, one above
   // (measured: 3.5% faster at 2^20-2^21 points, equal at 2^22, 3.5% slower from 2^23)
   acc_variant = group == ZKG_G1 ? ((double)max_entries < (double)(1u << 26) ? 3 : 4) : 2;
-  if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
 
   use(ctx);
   if (group == ZKG_G2) {
     set_acc_smem_limits();
     set_scan_smem_limits();
   }
+  layout();
+  result.alloc(xyzz_words(), "msm result");
+  result_handle.ctx = ctx;
+  result_handle.ptr = result.ptr;
+  result_handle.words = xyzz_words();
+  result_handle.owned = false;
+  check_cuda(cudaMemsetAsync(result.ptr, 0, xyzz_words() * 4, ctx->stream), "msm result init");
+}
+
+void MsmPlan::layout() {
+  const size_t np = points();
+  windows = glv ? (128 + c - 1) / c : (255 + c - 1) / c;
+  half = 1u << (c - 1);
+  slots = (size_t)windows * half;
+  seg_len = item_points_req ? item_points_req : auto_seg_len(np, windows);
+  const size_t xw = xyzz_words();
+  const size_t max_entries = (size_t)windows * np;
+  if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
+
   counts.alloc(slots, "msm counts");
   slot_start.alloc(slots + 1, "msm slot_start");
   cursor.alloc(slots, "msm cursor");
@@ -153,12 +167,8 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   runs[0].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   runs[1].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   window_sums.alloc((size_t)windows * xw, "msm window sums");
-  result.alloc(xw, "msm result");
-  result_handle.ctx = ctx;
-  result_handle.ptr = result.ptr;
-  result_handle.words = xw;
-  result_handle.owned = false;
-  check_cuda(cudaMemsetAsync(result.ptr, 0, xw * 4, ctx->stream), "msm result init");
+  if (glv) glv_bases.alloc(np * affine_words(), "msm GLV bases");
+  else glv_bases.release();
 }
 
 size_t MsmPlan::xyzz_words() const { return group == ZKG_G1 ? 32 : 64; }
@@ -177,7 +187,28 @@ void MsmPlan::check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const 
                         " points need " + std::to_string(need_b));
 }
 
+void MsmPlan::set_glv(bool enable) {
+  if (enable == glv) return;
+  if (enable) {
+    if (group != ZKG_G1) fail(ZKG_EINVAL, "GLV splitting is for G1 (the endomorphism (x, y) -> (beta x, y))");
+    if (c > 16) fail(ZKG_EINVAL, "GLV splitting needs a window size c <= 16, got " + std::to_string(c));
+    if (fixed_base) fail(ZKG_EINVAL, "GLV splitting and fixed-base tables do not combine");
+    if (2 * n >= (size_t)kNegBit) fail(ZKG_EINVAL, "a GLV MSM holds fewer than 2^30 points");
+  }
+  use(ctx);
+  const bool old = glv;
+  glv = enable;
+  try {
+    layout();
+  } catch (...) {
+    glv = old;
+    layout();
+    throw;
+  }
+}
+
 void MsmPlan::set_fixed_base(bool enable) {
+  if (enable && glv) fail(ZKG_EINVAL, "GLV splitting and fixed-base tables do not combine");
   if (enable && c > 16) fail(ZKG_EINVAL, "fixed-base tables need a window size c <= 16, got " + std::to_string(c));
   if (enable && (size_t)windows * n >= (size_t)kNegBit)
     fail(ZKG_EINVAL, "a fixed-base table holds fewer than 2^31 points");
@@ -200,25 +231,37 @@ void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, u
   check_launch("msm_fixed_base_table");
 }
 
+// The ranked sort's counting pass (msm_rank), plain or with the GLV split.
+template <int AGG>
+void MsmPlan::rank(const uint32_t* scalars, cudaStream_t s) {
+  const unsigned b256 = 256;
+  if (glv)
+    msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), n, c, windows, 0, counts.ptr,
+                                                                   digits.as<uint16_t>(), ranks.ptr);
+  else
+    msm_rank<AGG, false><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, n, c, windows, fixed_base, counts.ptr,
+                                                             digits.as<uint16_t>(), ranks.ptr);
+}
+
 template <class F>
 void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
   const unsigned b256 = 256;
   switch (which) {
     case kStageCount:
       check_cuda(cudaMemsetAsync(counts.ptr, 0, active_slots() * 4, s), "msm counts clear");
+      if (glv) {
+        msm_glv_bases<<<grid_for(n, b256), b256, 0, s>>>(bases, n, glv_bases.ptr);
+        check_launch("msm_glv_bases");
+      }
       if (ranked_sort()) {
         if (sort_agg == 0)
-          msm_rank<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                digits.as<uint16_t>(), ranks.ptr);
+          rank<0>(scalars, s);
         else if (sort_agg == 1)
-          msm_rank<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                digits.as<uint16_t>(), ranks.ptr);
+          rank<1>(scalars, s);
         else if (sort_agg == 2)
-          msm_rank<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                digits.as<uint16_t>(), ranks.ptr);
+          rank<2>(scalars, s);
         else
-          msm_rank<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, fixed_base, counts.ptr,
-                                                                digits.as<uint16_t>(), ranks.ptr);
+          rank<3>(scalars, s);
         check_launch("msm_rank");
       } else if (sort_agg == 1)
         msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
@@ -245,8 +288,8 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
     }
     case kStageScatter:
       if (ranked_sort()) {
-        const dim3 grid((unsigned)grid_for(n, b256), windows);
-        msm_place<<<grid, b256, 0, s>>>(digits.as<uint16_t>(), ranks.ptr, n, half, fixed_base, slot_start.ptr,
+        const dim3 grid((unsigned)grid_for(points(), b256), windows);
+        msm_place<<<grid, b256, 0, s>>>(digits.as<uint16_t>(), ranks.ptr, points(), half, fixed_base, slot_start.ptr,
                                         sorted.ptr);
         check_launch("msm_place");
         break;
@@ -256,6 +299,7 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       check_launch("msm_scatter");
       break;
     case kStageAccumulate:
+      if (glv) bases = glv_bases.ptr;
       if ((acc_variant == 5 || acc_variant == 6) && std::is_same<F, Fq>::value) {
         // G1 with the accumulator in shared memory, four blocks per SM
         const size_t acc_smem = f64_acc_smem<f64::FqD>(true);
@@ -398,6 +442,33 @@ std::vector<std::pair<std::string, double>> MsmPlan::profile(const zkg_buf* base
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return out;
+}
+
+// ------------------------------------------------------------------ GLV split check
+
+// out[10 i ..]: |k1| (4 words), |k2| (4 words), sign of k1, sign of k2, by glv::split_half.
+__global__ void glv_split_kernel(const uint32_t* __restrict__ scalars, size_t count, uint32_t* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  for (int h = 0; h < 2; h++) {
+    uint32_t s[8];
+    load_scalar(scalars, i, s);
+    const bool neg = glv::split_half(s, h == 1);
+    for (int k = 0; k < 4; k++) out[10 * i + 4 * h + k] = s[k];
+    out[10 * i + 8 + h] = neg ? 1u : 0u;
+  }
+}
+
+void glv_split(zkg_ctx* ctx, const uint32_t* scalars, size_t count, uint32_t* out) {
+  use(ctx);
+  DeviceArray in, res;
+  in.alloc(count * 8, "GLV split input");
+  res.alloc(count * 10, "GLV split output");
+  check_cuda(cudaMemcpyAsync(in.ptr, scalars, count * 32, cudaMemcpyHostToDevice, ctx->stream), "copy");
+  glv_split_kernel<<<grid_for(count, 128), 128, 0, ctx->stream>>>(in.ptr, count, res.ptr);
+  check_launch("glv_split_kernel");
+  check_cuda(cudaMemcpyAsync(out, res.ptr, count * 40, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+  check_cuda(cudaStreamSynchronize(ctx->stream), "GLV split");
 }
 
 // ------------------------------------------------------------------ base upload

@@ -14,6 +14,9 @@ void upload_bases(zkg_ctx* ctx, const uint32_t* xy, size_t words, bool mont256, 
 // out (windows * n points) <- the fixed-base table of n resident bases for window size c: row w
 // holds 2^(c w) P_i (windows = ceil(255 / c)); queued on the context stream.
 void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, uint32_t c, zkg_buf* out);
+// The device's GLV split of `count` host scalars (8 words each): per scalar |k1| and |k2| (4
+// words each) and their signs (1 word each), to host memory.
+void glv_split(zkg_ctx* ctx, const uint32_t* scalars, size_t count, uint32_t* out);
 
 struct MsmPlan {
   enum Stage {
@@ -49,12 +52,18 @@ struct MsmPlan {
   // pass records each digit's rank in its slot, the placing pass runs window by window;
   // msm_rank / msm_place). 1 is the default where it applies (c <= 16).
   int sort_form = 1;
-  bool ranked_sort() const { return fixed_base || (sort_form == 1 && c <= 16); }
+  bool ranked_sort() const { return fixed_base || glv || (sort_form == 1 && c <= 16); }
   // Fixed-base mode: `bases` of run() is a table from fixed_base_table() (windows * n points,
   // row w = 2^(c w) P_i), every window's digits share one set of 2^(c-1) buckets, and the
   // result is that set's running sum: no per-window reductions and no combination doublings.
   // Needs c <= 16 (the ranked sort).
   bool fixed_base = false;
+  // GLV mode (G1, c <= 16): every scalar splits as k1 + k2 lambda with 127-bit halves, and the
+  // MSM runs over the 2n points P_i, phi(P_i) (glv_bases, made from `bases` on every run) with
+  // ceil(128 / c) windows: the same number of bucket additions, half the windows, so half the
+  // reductions and half the combination doublings.
+  bool glv = false;
+  size_t points() const { return glv ? 2 * n : n; }
   size_t active_slots() const { return fixed_base ? half : slots; }
   uint32_t active_windows() const { return fixed_base ? 1u : windows; }
   size_t slots = 0, heads_max = 0;
@@ -64,6 +73,7 @@ struct MsmPlan {
 
   DeviceArray counts, slot_start, cursor, tile_sums, sorted, buckets;
   DeviceArray ranks, digits;  // the ranked sort's rank (32 bits) and digit (16 bits) per (window, point), window-major
+  DeviceArray glv_bases;      // GLV mode: P_0..P_{n-1}, phi(P_0)..phi(P_{n-1})
   DeviceArray heads[2], head_keys[2];
   DeviceArray tots, runs[2], window_sums, result;
   zkg_buf result_handle;
@@ -80,6 +90,7 @@ struct MsmPlan {
   size_t affine_words() const;
   void check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const;
   void set_fixed_base(bool enable);
+  void set_glv(bool enable);
   // Queues every stage on stream s (no host synchronisation).
   void enqueue(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
   void run(const zkg_buf* bases, const zkg_buf* scalars);
@@ -91,6 +102,12 @@ struct MsmPlan {
   void stage(int which, const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
   template <class FC>
   void tail_stage(int which, cudaStream_t s);
+  // Windows, slots, segments, merge and reduction levels and their scratch, for the current
+  // mode (points() and the scalar width); the result buffer is kept.
+  void layout();
+  template <int AGG>
+  void rank(const uint32_t* scalars, cudaStream_t s);
+  uint32_t item_points_req = 0;
 };
 
 }  // namespace zkg

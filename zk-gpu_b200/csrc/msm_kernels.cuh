@@ -166,6 +166,169 @@ __global__ void msm_scatter(const uint32_t* __restrict__ scalars, size_t n, uint
   }
 }
 
+// ------------------------------------------------------------------ GLV split (G1)
+//
+// BN254 G1 has the endomorphism phi(x, y) = (beta x, y), beta a cube root of unity in Fq, and
+// phi(P) = lambda P for every P of G1 (a group of prime order r) with lambda the matching cube
+// root of unity in Fr. A scalar splits as k = k1 + k2 lambda (mod r) with short k1, k2
+// (Gallant, Lambert, Vanstone, CRYPTO 2001), so sum k_i P_i = sum (k1_i P_i + k2_i phi(P_i)): an
+// MSM over 2n points whose scalars have 127-bit magnitudes, half the windows of the 254-bit one.
+//
+// Lattice split: v1 = (a1, b1), v2 = (a2, b2) are short vectors with a + b lambda = 0 (mod r) and
+// a1 b2 - a2 b1 = r (the extended Euclidean algorithm on (r, lambda)); c1 = round(b2 k / r), c2 =
+// round(-b1 k / r), k1 = k - c1 a1 - c2 a2, k2 = -c1 b1 - c2 b2. The roundings use g1 =
+// round(2^256 b2 / r) and g2 = round(2^256 (-b1) / r): c = floor((k g + 2^255) / 2^256) is within
+// 1/2 + k / 2^257 < 5/8 of the exact quotient for k < r, so (k1, k2) = -e1 v1 - e2 v2 with |e1|,
+// |e2| < 5/8, and |k1|, |k2| < 5/8 (a1 + a2) < 2^126.2 (a2 = -b1 < 2^64, b2 < 2^127). Signed
+// c-bit digits of such a magnitude need ceil(128 / c) windows: the top window's bits stay below
+// 2^(c - 1.8), so its digit never carries out.
+namespace glv {
+__device__ constexpr uint64_t kR[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull,
+                            0x30644e72e131a029ull};
+__device__ constexpr uint64_t kA1[2] = {0x8211bbeb7d4f1128ull, 0x6f4d8248eeb859fcull};
+__device__ constexpr uint64_t kB2[2] = {0x0be4e1541221250bull, 0x6f4d8248eeb859fdull};
+__device__ constexpr uint64_t kShort[1] = {0x89d3256894d213e3ull};  // a2 = -b1
+__device__ constexpr uint64_t kG1[3] = {0x5398fd0300ff6565ull, 0x4ccef014a773d2d2ull, 0x2ull};
+__device__ constexpr uint64_t kG2[2] = {0xd91d232ec7e0b3d7ull, 0x2ull};
+// beta = 0x30644e72e131a0295e6dd9e7e0acccb0c28f069fbb966e3de4bd44e5607cfd48 (beta^3 = 1 mod q,
+// paired with lambda = 0x30644e72e131a029048b6e193fd84104cc37a73fec2bc5e9b8ca0b2d36636f23 mod
+// r), here times 2^256 mod q (Montgomery form).
+__device__ constexpr uint32_t kBetaMont[8] = {0x13e80b9cu, 0x3350c88eu, 0xdb5e56b9u, 0x7dce557cu,
+                                   0xb615564au, 0x6001b4b8u, 0x020217e0u, 0x2682e617u};
+
+// The low L limbs of a * b (64-bit limbs, little-endian).
+template <int L, int LA, int LB>
+__device__ __forceinline__ void mul_lo(const uint64_t (&a)[LA], const uint64_t (&b)[LB], uint64_t (&r)[L]) {
+#pragma unroll
+  for (int k = 0; k < L; k++) r[k] = 0;
+#pragma unroll
+  for (int i = 0; i < LA; i++) {
+    uint64_t carry = 0;
+#pragma unroll
+    for (int j = 0; j < LB; j++) {
+      if (i + j < L) {
+        const uint64_t lo = a[i] * b[j], hi = __umul64hi(a[i], b[j]);
+        uint64_t t = r[i + j] + lo;
+        uint64_t cy = t < lo;
+        t += carry;
+        cy += t < carry;
+        r[i + j] = t;
+        carry = hi + cy;  // r + a b + carry < 2^128: no overflow
+      }
+    }
+    if (i + LB < L) r[i + LB] = carry;
+  }
+}
+
+// a - b mod 2^(64 L).
+template <int L>
+__device__ __forceinline__ void sub_mod(uint64_t (&a)[L], const uint64_t (&b)[L]) {
+  uint64_t borrow = 0;
+#pragma unroll
+  for (int i = 0; i < L; i++) {
+    const uint64_t x = a[i] - b[i];
+    const uint64_t b1 = a[i] < b[i];
+    a[i] = x - borrow;
+    borrow = b1 | (x < borrow);
+  }
+}
+
+// floor((k g + 2^255) / 2^256), taking the LC limbs of the quotient.
+template <int LG, int LC>
+__device__ __forceinline__ void round_quotient(const uint64_t (&k)[4], const uint64_t (&g)[LG], uint64_t (&c)[LC]) {
+  uint64_t p[4 + LG];
+  mul_lo<4 + LG>(k, g, p);
+  const uint64_t t = p[3] + (1ull << 63);
+  uint64_t carry = t < p[3];
+#pragma unroll
+  for (int i = 4; i < 4 + LG; i++) {
+    p[i] += carry;
+    carry = carry && p[i] == 0;
+  }
+#pragma unroll
+  for (int i = 0; i < LC; i++) c[i] = p[4 + i];
+}
+
+// s (8 words, any 256-bit value; reduced mod r first, which changes no multiple of a point of
+// G1) -> |k1| (second = false) or |k2| (second = true) in words 0..3, words 4..7 zero; returns
+// whether that half is negative.
+__device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
+  uint64_t k[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) k[i] = s[2 * i] | (uint64_t)s[2 * i + 1] << 32;
+#pragma unroll
+  for (int t = 0; t < 5; t++) {  // 2^256 < 6 r
+    uint64_t d[4] = {k[0], k[1], k[2], k[3]};
+    uint64_t borrow = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint64_t x = d[i] - kR[i];
+      const uint64_t b1 = d[i] < kR[i];
+      d[i] = x - borrow;
+      borrow = b1 | (x < borrow);
+    }
+    if (!borrow) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) k[i] = d[i];
+    }
+  }
+  uint64_t c1[2], c2[1];
+  round_quotient(k, kG1, c1);  // < b2 + 1 < 2^127
+  round_quotient(k, kG2, c2);  // < -b1 + 1 < 2^64
+  uint64_t v[3], t[3];
+  if (!second) {  // k1 = k - c1 a1 - c2 a2
+    v[0] = k[0];
+    v[1] = k[1];
+    v[2] = k[2];
+    mul_lo<3>(c1, kA1, t);
+    sub_mod(v, t);
+    mul_lo<3>(c2, kShort, t);
+    sub_mod(v, t);
+  } else {  // k2 = c1 (-b1) - c2 b2
+    mul_lo<3>(c1, kShort, v);
+    mul_lo<3>(c2, kB2, t);
+    sub_mod(v, t);
+  }
+  const bool neg = v[2] >> 63;
+  if (neg) {
+    const uint64_t zero[3] = {0, 0, 0};
+    uint64_t m[3] = {zero[0], zero[1], zero[2]};
+    sub_mod(m, v);
+    v[0] = m[0];
+    v[1] = m[1];
+  }
+  s[0] = (uint32_t)v[0];
+  s[1] = (uint32_t)(v[0] >> 32);
+  s[2] = (uint32_t)v[1];
+  s[3] = (uint32_t)(v[1] >> 32);
+#pragma unroll
+  for (int i = 4; i < 8; i++) s[i] = 0;
+  return neg;
+}
+}  // namespace glv
+
+// The 2n bases of a GLV MSM: out[i] = P_i, out[n + i] = phi(P_i) = (beta x_i, y_i), affine in
+// Montgomery form (infinity, (0, 0), stays (0, 0)).
+__global__ void msm_glv_bases(const uint32_t* __restrict__ bases, size_t n, uint32_t* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint4* src = reinterpret_cast<const uint4*>(bases + 16 * i);
+  const uint4 x0 = __ldg(src), x1 = __ldg(src + 1), y0 = __ldg(src + 2), y1 = __ldg(src + 3);
+  uint4* lo = reinterpret_cast<uint4*>(out + 16 * i);
+  lo[0] = x0;
+  lo[1] = x1;
+  lo[2] = y0;
+  lo[3] = y1;
+  Fq beta;
+#pragma unroll
+  for (int k = 0; k < 8; k++) beta.w[k] = glv::kBetaMont[k];
+  const Fq bx = load_fe<Fq>(bases + 16 * i) * beta;
+  store_fe(out + 16 * (n + i), bx);
+  uint4* hi = reinterpret_cast<uint4*>(out + 16 * (n + i));
+  hi[2] = y0;
+  hi[3] = y1;
+}
+
 // ------------------------------------------------------------------ ranked counting sort
 //
 // The same sort in two passes without scattered stores over the whole sorted array:
@@ -182,14 +345,25 @@ constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occ
 
 // fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
 // window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
-template <int AGG>
-__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows, int fixed,
-                         uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
+// GLV: n = 2 scalar_n points; entry i < scalar_n takes |k1| of scalar i, entry scalar_n + i
+// takes |k2| of scalar i (glv::split_half), each half's sign folded into its digits' signs.
+template <int AGG, bool GLV = false>
+__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t scalar_n, uint32_t c, uint32_t windows,
+                         int fixed, uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
                          uint32_t* __restrict__ ranks) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
   Recoder rc;
-  if (live) load_scalar(scalars, i, rc.s);
+  bool flip = false;
+  if (live) {
+    if (GLV) {
+      const bool second = i >= scalar_n;
+      load_scalar(scalars, second ? i - scalar_n : i, rc.s);
+      flip = glv::split_half(rc.s, second);
+    } else {
+      load_scalar(scalars, i, rc.s);
+    }
+  }
   const uint32_t half = 1u << (c - 1);
   const unsigned lane = threadIdx.x & 31;
   // Windows four at a time: the four counting atomics (each returns the entry's rank) are in
@@ -222,7 +396,7 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_
       uint32_t code = kRankZero;
       const size_t e = (size_t)w * n + i;
       if (peers[k]) {
-        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);
+        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] != flip ? 0x8000u : 0u);
         __stcs(ranks + e, b + __popc(peers[k] & ((1u << lane) - 1)));  // streamed: read once by msm_place
       }
       __stcs(digits + e, (unsigned short)code);

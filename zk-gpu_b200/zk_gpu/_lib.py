@@ -73,6 +73,8 @@ SIGNATURES = {
     "zkg_msm_fixed_base_table": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.c_uint32,
                                                 ctypes.POINTER(vp)]),
     "zkg_msm_set_fixed_base": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_set_glv": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_windows": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int)]),
     "zkg_xyzz_add_host": (ctypes.c_int, [ctypes.c_int, u32p, u32p, u32p]),
     "zkg_quotient": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32, u32p]),
     "zkg_zkey_parse": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(vp)]),
@@ -136,6 +138,7 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     "zkg_bench_integer_pipe": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "zkg_test_point_ops": (ctypes.c_int, [vp, ctypes.c_int, u32p, ctypes.c_size_t, u32p]),
+    "zkg_test_glv_split": (ctypes.c_int, [vp, u32p, ctypes.c_size_t, u32p]),
     "zkg_generator_multiples": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.c_int, vp]),
 }
 

@@ -83,6 +83,17 @@ class Msm:
         check(lib().zkg_msm_fixed_base_table(gpu.handle, int(group), bases.handle, n, c, ctypes.byref(h)))
         return Buffer(gpu, h.value)
 
+    def set_glv(self, enable: bool = True) -> None:
+        """G1: split every scalar as k1 + k2 lambda (mod r) and run over P_i and phi(P_i) with
+        ceil(128 / c) windows; the same result as the plain MSM."""
+        check(lib().zkg_msm_set_glv(self._h, int(enable)))
+
+    def windows(self) -> tuple[int, bool]:
+        """(window count, GLV on)."""
+        w, g = ctypes.c_uint32(), ctypes.c_int()
+        check(lib().zkg_msm_windows(self._h, ctypes.byref(w), ctypes.byref(g)))
+        return w.value, bool(g.value)
+
     def set_sort_form(self, form: int) -> None:
         """Counting sort: 0 scatter through atomic cursors, 1 ranked placement window by window
         (default for c <= 16)."""
