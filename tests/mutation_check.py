@@ -30,7 +30,7 @@ MUTANTS = [
     ("digits-mask", CSRC + "msm_kernels.cuh", "  return v & ((1u << c) - 1);\n}", "  return v & ((1u << c) - 2);\n}"),
     ("combine-shift", CSRC + "msm_kernels.cuh", "for (uint32_t k = 0; k < c; k++) acc = lane_double(acc, sm);",
      "for (uint32_t k = 1; k < c; k++) acc = lane_double(acc, sm);"),
-    ("sort-sign", CSRC + "msm_kernels.cuh", "code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] != flip ? 0x8000u : 0u);",
+    ("sort-sign", CSRC + "msm_kernels.cuh", "code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);",
      "code = (fixed ? slot[k] : slot[k] - w * half) | 0u;"),
     ("reduce-weights", CSRC + "msm_kernels.cuh",
      "      if (!empty) run = xyzz_add(run, load_xyzz<F>(in + slot * XW));\n      tot = xyzz_add(tot, run);",

@@ -233,14 +233,15 @@ void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, u
 
 // The ranked sort's counting pass (msm_rank), plain or with the GLV split.
 template <int AGG>
-void MsmPlan::rank(const uint32_t* scalars, cudaStream_t s) {
+void MsmPlan::rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
   const unsigned b256 = 256;
   if (glv)
     msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), n, c, windows, 0, counts.ptr,
-                                                                   digits.as<uint16_t>(), ranks.ptr);
+                                                                   digits.as<uint16_t>(), ranks.ptr, bases,
+                                                                   glv_bases.ptr);
   else
     msm_rank<AGG, false><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, n, c, windows, fixed_base, counts.ptr,
-                                                             digits.as<uint16_t>(), ranks.ptr);
+                                                             digits.as<uint16_t>(), ranks.ptr, nullptr, nullptr);
 }
 
 template <class F>
@@ -249,19 +250,15 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
   switch (which) {
     case kStageCount:
       check_cuda(cudaMemsetAsync(counts.ptr, 0, active_slots() * 4, s), "msm counts clear");
-      if (glv) {
-        msm_glv_bases<<<grid_for(n, b256), b256, 0, s>>>(bases, n, glv_bases.ptr);
-        check_launch("msm_glv_bases");
-      }
       if (ranked_sort()) {
         if (sort_agg == 0)
-          rank<0>(scalars, s);
+          rank<0>(bases, scalars, s);
         else if (sort_agg == 1)
-          rank<1>(scalars, s);
+          rank<1>(bases, scalars, s);
         else if (sort_agg == 2)
-          rank<2>(scalars, s);
+          rank<2>(bases, scalars, s);
         else
-          rank<3>(scalars, s);
+          rank<3>(bases, scalars, s);
         check_launch("msm_rank");
       } else if (sort_agg == 1)
         msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);

@@ -59,9 +59,11 @@ struct MsmPlan {
   // Needs c <= 16 (the ranked sort).
   bool fixed_base = false;
   // GLV mode (G1, c <= 16): every scalar splits as k1 + k2 lambda with 127-bit halves, and the
-  // MSM runs over the 2n points P_i, phi(P_i) (glv_bases, made from `bases` on every run) with
+  // MSM runs over the 2n points +-P_i, +-phi(P_i) (glv_bases, made from `bases` on every run) with
   // ceil(128 / c) windows: the same number of bucket additions, half the windows, so half the
-  // reductions and half the combination doublings.
+  // reductions and half the combination doublings. The counting pass writes glv_bases, each
+  // base carrying its half-scalar's sign: the digits' 16-bit codes (kRankZero) have no room for
+  // a sign flip at c = 16.
   bool glv = false;
   size_t points() const { return glv ? 2 * n : n; }
   size_t active_slots() const { return fixed_base ? half : slots; }
@@ -106,7 +108,7 @@ struct MsmPlan {
   // mode (points() and the scalar width); the result buffer is kept.
   void layout();
   template <int AGG>
-  void rank(const uint32_t* scalars, cudaStream_t s);
+  void rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
   uint32_t item_points_req = 0;
 };
 

@@ -307,26 +307,21 @@ __device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
 }
 }  // namespace glv
 
-// The 2n bases of a GLV MSM: out[i] = P_i, out[n + i] = phi(P_i) = (beta x_i, y_i), affine in
-// Montgomery form (infinity, (0, 0), stays (0, 0)).
-__global__ void msm_glv_bases(const uint32_t* __restrict__ bases, size_t n, uint32_t* __restrict__ out) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint4* src = reinterpret_cast<const uint4*>(bases + 16 * i);
-  const uint4 x0 = __ldg(src), x1 = __ldg(src + 1), y0 = __ldg(src + 2), y1 = __ldg(src + 3);
-  uint4* lo = reinterpret_cast<uint4*>(out + 16 * i);
-  lo[0] = x0;
-  lo[1] = x1;
-  lo[2] = y0;
-  lo[3] = y1;
-  Fq beta;
+// Base of GLV entry i (point src = i mod n; second: the k2 half): P_src or phi(P_src) = (beta x,
+// y), negated ((x, q - y)) when that half of the scalar is negative, so the digits keep their own
+// signs. Affine, Montgomery form; infinity, (0, 0), stays (0, 0).
+__device__ __forceinline__ void glv_base(const uint32_t* __restrict__ bases, size_t src, bool second, bool neg,
+                                         uint32_t* __restrict__ out) {
+  Fq x = load_fe<Fq>(bases + 16 * src), y = load_fe<Fq>(bases + 16 * src + 8);
+  if (second) {
+    Fq beta;
 #pragma unroll
-  for (int k = 0; k < 8; k++) beta.w[k] = glv::kBetaMont[k];
-  const Fq bx = load_fe<Fq>(bases + 16 * i) * beta;
-  store_fe(out + 16 * (n + i), bx);
-  uint4* hi = reinterpret_cast<uint4*>(out + 16 * (n + i));
-  hi[2] = y0;
-  hi[3] = y1;
+    for (int k = 0; k < 8; k++) beta.w[k] = glv::kBetaMont[k];
+    x = x * beta;
+  }
+  if (neg && !y.is_zero()) y = Fq::zero() - y;
+  store_fe(out, x);
+  store_fe(out + 8, y);
 }
 
 // ------------------------------------------------------------------ ranked counting sort
@@ -346,20 +341,23 @@ constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occ
 // fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
 // window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
 // GLV: n = 2 scalar_n points; entry i < scalar_n takes |k1| of scalar i, entry scalar_n + i
-// takes |k2| of scalar i (glv::split_half), each half's sign folded into its digits' signs.
+// takes |k2| of scalar i (glv::split_half), and glv_bases[i] gets the matching base with that
+// half's sign (glv_base).
 template <int AGG, bool GLV = false>
 __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t scalar_n, uint32_t c, uint32_t windows,
                          int fixed, uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
-                         uint32_t* __restrict__ ranks) {
+                         uint32_t* __restrict__ ranks, const uint32_t* __restrict__ bases,
+                         uint32_t* __restrict__ glv_bases) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
   Recoder rc;
-  bool flip = false;
   if (live) {
     if (GLV) {
       const bool second = i >= scalar_n;
-      load_scalar(scalars, second ? i - scalar_n : i, rc.s);
-      flip = glv::split_half(rc.s, second);
+      const size_t src = second ? i - scalar_n : i;
+      load_scalar(scalars, src, rc.s);
+      const bool neg = glv::split_half(rc.s, second);
+      glv_base(bases, src, second, neg, glv_bases + 16 * i);
     } else {
       load_scalar(scalars, i, rc.s);
     }
@@ -396,7 +394,7 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t 
       uint32_t code = kRankZero;
       const size_t e = (size_t)w * n + i;
       if (peers[k]) {
-        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] != flip ? 0x8000u : 0u);
+        code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);
         __stcs(ranks + e, b + __popc(peers[k] & ((1u << lane) - 1)));  // streamed: read once by msm_place
       }
       __stcs(digits + e, (unsigned short)code);
