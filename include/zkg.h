@@ -151,9 +151,10 @@ int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
 /* GLV splitting for G1 (no reference counterpart; the reference names GLV as a next step,
  * README.md:223-224): with enable = 1 every scalar k is split as k1 + k2 lambda (mod r), |k1|,
  * |k2| < 2^127, and a run sums k1_i P_i + k2_i phi(P_i) with phi(x, y) = (beta x, y): 2n points
- * (the plan makes phi(P_i) from `bases` on every run, 128 more bytes of plan memory per point)
- * with ceil(128 / c) windows instead of ceil(255 / c), so the same number of bucket additions
- * and half the bucket reductions and combination doublings. The result is the same point as the
+ * (the plan makes +-phi(P_i) from `bases` on every run, 128 more bytes of plan memory per point)
+ * with W = ceil(128 / c) windows instead of ceil(255 / c), the 128 bits spread over them as
+ * evenly as possible (widths floor(128 / W) or one more, never above c), so about the same number
+ * of bucket additions and half the bucket reductions and combination doublings. The result is the same point as the
  * plain MSM (scalars are taken mod r). Needs G1, c <= 16, no fixed-base table and n < 2^30;
  * otherwise ZKG_EINVAL. Re-sizes the plan's scratch (synchronises with queued work).
  * zkg_msm_windows reports the plan's window count and whether GLV is on. */

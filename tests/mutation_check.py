@@ -26,10 +26,14 @@ CSRC = "zk-gpu_b200/csrc/"
 
 # (name, file, text to find, replacement). The text must occur exactly once in the file.
 MUTANTS = [
-    ("digits-carry", CSRC + "msm_kernels.cuh", "      *neg = true;\n      carry = 1;", "      *neg = true;"),
+    ("digits-carry", CSRC + "msm_kernels.cuh", "      mag = (1u << c) - v;\n      *neg = true;\n      carry = 1;",
+     "      mag = (1u << c) - v;\n      *neg = true;"),
     ("digits-mask", CSRC + "msm_kernels.cuh", "  return v & ((1u << c) - 1);\n}", "  return v & ((1u << c) - 2);\n}"),
-    ("combine-shift", CSRC + "msm_kernels.cuh", "for (uint32_t k = 0; k < c; k++) acc = lane_double(acc, sm);",
-     "for (uint32_t k = 1; k < c; k++) acc = lane_double(acc, sm);"),
+    ("combine-shift", CSRC + "msm_kernels.cuh", "for (uint32_t k = 0; k < width; k++) acc = lane_double(acc, sm);",
+     "for (uint32_t k = 1; k < width; k++) acc = lane_double(acc, sm);"),
+    ("glv-round", CSRC + "msm_kernels.cuh", "const uint64_t t = p[3] + (1ull << 63);", "const uint64_t t = p[3];"),
+    ("glv-sign", CSRC + "msm_kernels.cuh", "if (neg && !y.is_zero()) y = Fq::zero() - y;",
+     "if (false && neg && !y.is_zero()) y = Fq::zero() - y;"),
     ("sort-sign", CSRC + "msm_kernels.cuh", "code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);",
      "code = (fixed ? slot[k] : slot[k] - w * half) | 0u;"),
     ("reduce-weights", CSRC + "msm_kernels.cuh",

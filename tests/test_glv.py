@@ -64,6 +64,19 @@ def test_split_is_exact_and_short():
         assert abs(k1) < bound and abs(k2) < bound, hex(k)
 
 
+def test_window_widths():
+    """The GLV windows (glv_window_pos / glv_window_width in msm_kernels.cuh): W = ceil(128 / c)
+    windows cover bits 0..127 exactly, none wider than c (their digits fit the plan's 2^(c-1)
+    buckets), and the top one is wide enough that a half below 2^126.2 leaves its digit below
+    half its range (no carry out of the last window)."""
+    for c in range(9, 17):
+        w = -(-128 // c)
+        widths = [128 // w + (1 if i < 128 % w else 0) for i in range(w)]
+        assert sum(widths) == 128 and max(widths) <= c, c
+        top = widths[-1]
+        assert 2 ** (126.2 - (128 - top)) + 1 < 2 ** (top - 1), c
+
+
 # ---------------------------------------------------------------- the split (GPU)
 
 @pytest.mark.gpu

@@ -331,7 +331,9 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
     case kStageCombine:
       // c (W - 1) dependent doublings: one warp, each level's independent products on separate
       // lanes (one out-of-line product per lane).
-      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), c,
+      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
+                                                                       glv ? 128u / windows : c,
+                                                                       glv ? 128u % windows : 0u,
                                                                        result.ptr);
       check_launch("msm_combine_lanes");
       break;

@@ -60,8 +60,9 @@ struct MsmPlan {
   bool fixed_base = false;
   // GLV mode (G1, c <= 16): every scalar splits as k1 + k2 lambda with 127-bit halves, and the
   // MSM runs over the 2n points +-P_i, +-phi(P_i) (glv_bases, made from `bases` on every run) with
-  // ceil(128 / c) windows: the same number of bucket additions, half the windows, so half the
-  // reductions and half the combination doublings. The counting pass writes glv_bases, each
+  // W = ceil(128 / c) windows of floor(128 / W) or floor(128 / W) + 1 bits (glv_window_width):
+  // about the same number of bucket additions, half the windows, so half the reductions and half
+  // the combination doublings. The counting pass writes glv_bases, each
   // base carrying its half-scalar's sign: the digits' 16-bit codes (kRankZero) have no room for
   // a sign flip at c = 16.
   bool glv = false;

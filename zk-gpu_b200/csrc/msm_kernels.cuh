@@ -77,7 +77,34 @@ struct Recoder {
     }
     return mag ? w * half + mag - 1 : kNoKey;
   }
+  // The same for a window of `width` bits starting at bit `pos` (width <= c: the GLV windows).
+  __device__ __forceinline__ uint32_t next_at(uint32_t w, uint32_t pos, uint32_t width, uint32_t half, bool* neg) {
+    uint32_t v = window_bits(s, pos, width) + carry;
+    carry = 0;
+    uint32_t mag = v;
+    *neg = false;
+    if (v >= (1u << (width - 1))) {
+      mag = (1u << width) - v;
+      *neg = true;
+      carry = 1;
+    }
+    return mag ? w * half + mag - 1 : kNoKey;
+  }
 };
+
+// GLV windows: the 128 bits of the halves split as evenly as possible over W windows, the first
+// 128 mod W of them floor(128 / W) + 1 bits wide and the rest floor(128 / W) (at most c bits
+// each, since W = ceil(128 / c)). Equal c-bit windows would leave the top one with as little as
+// 0.2 significant bits (|k| < 2^126.2), whose few buckets would take every entry's counting
+// atomic; here every window keeps at least floor(128 / W) - 1.8 bits, and the top one still
+// cannot carry out.
+__device__ __forceinline__ uint32_t glv_window_pos(uint32_t w, uint32_t windows) {
+  const uint32_t base = 128u / windows, extra = 128u % windows;
+  return w * base + (w < extra ? w : extra);
+}
+__device__ __forceinline__ uint32_t glv_window_width(uint32_t w, uint32_t windows) {
+  return 128u / windows + (w < 128u % windows ? 1u : 0u);
+}
 
 // Lanes of a warp that share a slot, for one atomic per group. AGG 0: every group
 // (__match_any_sync); 1: only the group of the first lane that has a slot (one shuffle and one
@@ -377,7 +404,9 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t 
       slot[k] = kNoKey;
       neg[k] = false;
       if (w < windows) {  // uniform across the warp
-        if (live) slot[k] = rc.next(w, c, half, &neg[k]);
+        if (live)
+          slot[k] = GLV ? rc.next_at(w, glv_window_pos(w, windows), glv_window_width(w, windows), half, &neg[k])
+                        : rc.next(w, c, half, &neg[k]);
         if (fixed && slot[k] != kNoKey) slot[k] -= w * half;
         peers[k] = slot_peers<AGG>(slot[k]);
         base[k] = 0;
@@ -804,18 +833,21 @@ __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t
   if (threadIdx.x == 0) store_xyzz(window_sums + (size_t)w * XW, acc);
 }
 
-// result = sum_w 2^(c*w) S_w by Horner from the top window (msm_combine.wgsl:13-22), by one
-// warp: each level's independent products run on separate lanes (curve_lanes.cuh). F is the
+// result = sum_w 2^(pos_w) S_w by Horner from the top window (msm_combine.wgsl:13-22), by one
+// warp: each level's independent products run on separate lanes (curve_lanes.cuh). Window w is
+// `base` bits wide, or base + 1 for w < extra (pos_w is the sum of the widths below w): base =
+// c, extra = 0 for the plain windows, the glv_window_width split for GLV. F is the
 // one-product-per-call form (FqC or Fq2C).
 template <class F>
 __global__ void __launch_bounds__(32) msm_combine_lanes(const uint32_t* __restrict__ window_sums, uint32_t windows,
-                                                        uint32_t c, uint32_t* __restrict__ result) {
+                                                        uint32_t base, uint32_t extra, uint32_t* __restrict__ result) {
   __shared__ uint32_t scratch[32 * 8];
   const LaneScratch sm{scratch};
   constexpr int XW = PointWords<F>::xyzz;
   Xyzz<F> acc = load_xyzz<F>(window_sums + (size_t)(windows - 1) * XW);
   for (int w = (int)windows - 2; w >= 0; w--) {
-    for (uint32_t k = 0; k < c; k++) acc = lane_double(acc, sm);
+    const uint32_t width = base + ((uint32_t)w < extra ? 1u : 0u);
+    for (uint32_t k = 0; k < width; k++) acc = lane_double(acc, sm);
     acc = lane_add(acc, load_xyzz<F>(window_sums + (size_t)w * XW), sm);
   }
   if (threadIdx.x == 0) store_xyzz(result, acc);
