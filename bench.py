@@ -378,6 +378,7 @@ def run_ours(a, d: Dist) -> dict | None:
             "workload": workload_name(a),
             "parallelism": f"replicas x{d.world} (one full step per GPU)",
             "windows": {"msm_2^%d" % a.log_msm: c24, "msm_2^%d" % a.log_msm_small: c20},
+            "msm_plans": {f"msm_2^{a.log_msm}": msm24.params(), f"msm_2^{a.log_msm_small}": msm20.params()},
             "l2": "inputs larger than L2 (2^24 MSM bases 1 GiB, scalars 512 MiB; NTT 512 MiB); no flush",
         },
         "parts_ms": {

@@ -155,9 +155,11 @@ int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
  * with W = ceil(128 / c) windows instead of ceil(255 / c), the 128 bits spread over them as
  * evenly as possible (widths floor(128 / W) or one more, never above c), so about the same number
  * of bucket additions and half the bucket reductions and combination doublings. The result is the same point as the
- * plain MSM (scalars are taken mod r). Needs G1, c <= 16, no fixed-base table and n < 2^30;
- * otherwise ZKG_EINVAL. Re-sizes the plan's scratch (synchronises with queued work).
- * zkg_msm_windows reports the plan's window count and whether GLV is on. */
+ * plain MSM (scalars are taken mod r). On by default for G1 plans with c <= 16 and n < 2^30
+ * (measured faster at every default window); enable = 1 elsewhere (G2, c > 16, a fixed-base
+ * plan) is ZKG_EINVAL; zkg_msm_set_fixed_base(msm, 1) switches it off. Re-sizes the plan's
+ * scratch (synchronises with queued work). zkg_msm_windows reports the plan's window count and
+ * whether GLV is on. */
 int zkg_msm_set_glv(zkg_msm *msm, int enable);
 int zkg_msm_windows(const zkg_msm *msm, uint32_t *windows, int *glv);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
@@ -261,7 +263,8 @@ int zkg_zkey_upload(zkg_ctx *ctx, const zkg_zkey *zkey, uint32_t section, zkg_bu
 /* ------------------------------------------------------------------ autotuning
  * No reference counterpart (its parameters are fixed: default_window, item size, TILE_LOG).
  * zkg_tune_msm times, on the given inputs, windows c in [default_window(n) - 2, + 2] within
- * 9..=20, 16..256 points per accumulation thread and the three accumulation kernel forms, and writes
+ * 9..=20, 16..256 points per accumulation thread, the accumulation kernel forms and, for G1 with
+ * c <= 16, the GLV split on and off, and writes
  * up to cap results fastest first (out[0] is the choice; *count receives how many).
  * zkg_ntt_set_variant picks a plan's butterfly form: 0 = 32-bit integer products (tiles of 2^11
  * elements; default), 1 = double-precision limbs, products on the FP64 pipe (tiles of 2^10);
@@ -273,6 +276,7 @@ int zkg_zkey_upload(zkg_ctx *ctx, const zkg_zkey *zkey, uint32_t section, zkg_bu
 typedef struct {
   uint32_t c, item_points;
   int variant;
+  int glv; /* zkg_msm_set_glv */
   double ms;
 } zkg_msm_tuning;
 int zkg_tune_msm(zkg_ctx *ctx, int group, size_t n, const zkg_buf *bases, const zkg_buf *scalars, int reps,

@@ -193,9 +193,10 @@ def test_full_size_distributions(gpu, log_n, kind):
 
 
 @pytest.mark.gpu
-def test_full_size_2_24(gpu):
+@pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"] if not quick() else ["uniform"])
+def test_full_size_2_24(gpu, kind):
     from test_msm import full_size_case
-    full_size_case(gpu, 24, "uniform", glv=True)
+    full_size_case(gpu, 24, kind, glv=True)
 
 
 @pytest.mark.gpu
@@ -204,22 +205,22 @@ def test_switching_and_checks(gpu):
     bases, scalars = random_points("G1", 40, n), random_fr(41, n)
     want = msm_ref("G1", bases, scalars)
     msm = Msm(gpu, n, 12)
-    assert msm.windows() == (22, False)
+    assert msm.windows() == (11, True)  # the G1 default where it applies
     base_buf, scalar_buf = Msm.upload_bases(gpu, bases), gpu.buffer(scalars)
     from zk_gpu import xyzz_to_affine
     from zk_gpu.msm import affine_words
-    for glv, windows in ((True, 11), (False, 22), (True, 11)):
+    for glv, windows in ((False, 22), (True, 11), (False, 22), (True, 11)):
         msm.set_glv(glv)
         assert msm.windows() == (windows, glv)
         got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, scalar_buf), 32)))
         assert np.array_equal(got, want), f"GLV {glv}"
+    assert Msm.for_group(gpu, Group.G2, 1024, 10).windows() == (26, False)
+    assert Msm(gpu, 1024, 17).windows() == (15, False)
     with pytest.raises(ZkGpuError, match="GLV splitting is for G1"):
         Msm.for_group(gpu, Group.G2, 1024, 10).set_glv(True)
     with pytest.raises(ZkGpuError, match=r"GLV splitting needs a window size c <= 16, got 17"):
         Msm(gpu, 1024, 17).set_glv(True)
-    with pytest.raises(ZkGpuError, match="do not combine"):
-        msm.set_fixed_base(True)
-    msm.set_glv(False)
-    msm.set_fixed_base(True)
+    msm.set_fixed_base(True)  # switches GLV off: a table's rows are the plain windows
+    assert msm.windows() == (22, False)
     with pytest.raises(ZkGpuError, match="do not combine"):
         msm.set_glv(True)

@@ -17,11 +17,13 @@ R = bn254.R
 
 
 def check(gpu, bases, scalars, c, what, variant=None):
+    """Both the plain windows and the default (the GLV split for G1, c <= 16)."""
     expected = msm_ref("G1", bases, scalars)
     for item_points in (1024, 7):
-        got = gpu_msm(gpu, bases, scalars, (c, item_points), variant=variant)
-        assert np.array_equal(got, expected), \
-            f"{what} (n = {scalars.size // 8}, c = {c}, item_points = {item_points}, variant = {variant})"
+        for glv in (False, None):
+            got = gpu_msm(gpu, bases, scalars, (c, item_points), variant=variant, glv=glv)
+            assert np.array_equal(got, expected), \
+                f"{what} (n = {scalars.size // 8}, c = {c}, item_points = {item_points}, variant = {variant}, glv = {glv})"
 
 
 # Accumulation kernel forms checked by the edge-case suites: the default, and the G1 forms
@@ -236,10 +238,11 @@ def fuzz_case(gpu, seed):
     else:
         s = fr_words([0, 1, R - 1][int(v)] for v in rnd.integers(0, 3, size=n))
     bases = np.ascontiguousarray(bases.reshape(-1))
-    got = gpu_msm(gpu, bases, s, (c, item_points))
+    glv = bool(rnd.integers(0, 2))
+    got = gpu_msm(gpu, bases, s, (c, item_points), glv=glv)
     assert np.array_equal(got, msm_ref("G1", bases, s)), (
         f"FUZZ FAILURE: rerun with ZK_GPU_FUZZ_SEED={seed} (n={n}, c={c}, item_points={item_points}, "
-        f"scalars={scalar_kind}, bases={base_kind})")
+        f"scalars={scalar_kind}, bases={base_kind}, glv={glv})")
 
 
 def fuzz_forms_case(gpu, seed):
@@ -270,7 +273,8 @@ def fuzz_forms_case(gpu, seed):
     bases = np.ascontiguousarray(bases.reshape(-1))
     want = msm_ref(g, bases, s)
     for variant in (1, 2, 3, 4):
-        got = gpu_msm(gpu, bases, s, (c, item_points), group=group, variant=variant)
+        got = gpu_msm(gpu, bases, s, (c, item_points), group=group, variant=variant,
+                      glv=bool(variant & 1) if g == "G1" else None)
         assert np.array_equal(got, want), (
             f"seed {seed}: {g} n={n} c={c} item_points={item_points} bases={kind} scalars={sk} form {variant}")
 
@@ -327,12 +331,12 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant
 @pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"])
 @pytest.mark.parametrize("log_n", [18, 20, 22])
 def test_full_size_distributions(gpu, log_n, kind):
-    full_size_case(gpu, log_n, kind)
+    full_size_case(gpu, log_n, kind, glv=False)  # the plain windows (GLV: tests/test_glv.py)
 
 
 @pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"] if not quick() else ["uniform"])
 def test_full_size_2_24(gpu, kind):
-    full_size_case(gpu, 24, kind)
+    full_size_case(gpu, 24, kind, glv=False)
 
 
 @pytest.mark.parametrize("kind", ["uniform", "sparse", "r-1"])
@@ -379,6 +383,7 @@ def test_autotuned_plan_is_exact(gpu, tmp_path, monkeypatch):
     results = search_msm(gpu, Group.G1, n, bb, sb, reps=1)
     assert results and results == sorted(results, key=lambda r: r["ms"])
     assert {r["variant"] for r in results} == {1, 2, 3, 4}
+    assert {r["glv"] for r in results} == {0, 1}
     msm = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)
     again = tuned_msm(gpu, Group.G1, n, bb, sb, reps=1)  # from the cache
     assert msm.params() == again.params()

@@ -65,7 +65,10 @@ struct MsmPlan {
   // the combination doublings. The counting pass writes glv_bases, each
   // base carrying its half-scalar's sign: the digits' 16-bit codes (kRankZero) have no room for
   // a sign flip at c = 16.
+  // On by default where it applies (glv_default); zkg_msm_set_glv switches it; fixed-base mode
+  // switches it off.
   bool glv = false;
+  bool glv_default() const;
   size_t points() const { return glv ? 2 * n : n; }
   size_t active_slots() const { return fixed_base ? half : slots; }
   uint32_t active_windows() const { return fixed_base ? 1u : windows; }

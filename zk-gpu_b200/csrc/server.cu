@@ -114,11 +114,16 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
   const size_t m = (size_t)1 << log_m, N = 2 * m;
   auto msm = [&](size_t xw) {
     const uint32_t c = default_window(m), W = (255 + c - 1) / c;
+    const bool glv = xw == 32 && c <= 16;  // G1 plans split with GLV by default
+    const uint32_t Wg = (128 + c - 1) / c;
     const size_t B = (size_t)1 << (c - 1), S = (size_t)W * B;
-    const size_t entries = (size_t)W * m, L = 8;  // worst case of the automatic segment length
+    // (point, window) entries: the GLV plan has Wg windows over 2m points
+    const size_t entries = std::max((size_t)W * m, glv ? (size_t)Wg * 2 * m : 0), L = 8;  // worst-case segment
     const size_t heads = entries / L + 1;
-    // counts, slot starts, cursors; sorted entries, ranks and digits; buckets; heads; running sums
-    return 4 * (3 * S + entries * 5 / 2 + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 + 4096);
+    // counts, slot starts, cursors; sorted entries, ranks and digits; buckets; heads; running
+    // sums; the GLV bases (2m affine points)
+    return 4 * (3 * S + entries * 5 / 2 + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 +
+                (glv ? 2 * m * 16 : 0) + 4096);
   };
   // scratch, twiddle words (both directions), staged twiddle tables (both directions: 40 bytes
   // per element for the first pass, at most as much again for the later passes' small tables

@@ -4,7 +4,8 @@
 // (examples/g2_window.rs:50-69); default_window stays the plain form beside the tuned one.
 //
 // MSM candidates: window c in [default - 2, default + 2] within 9..=20, points per accumulation
-// thread in {16, 32, 64, 128, 256}, both accumulation kernel forms. NTT candidates: the most
+// thread in {16, 32, 64, 128, 256}, the accumulation kernel forms, and for G1 (c <= 16) the GLV
+// split on and off. NTT candidates: the most
 // stages per shared-memory pass (passes = ceil(log_n / max_stages)). Each candidate runs once to
 // warm up, then `reps` times between CUDA events; the best mean wins.
 #include <algorithm>
@@ -39,28 +40,33 @@ std::vector<zkg_msm_tuning> tune_msm(zkg_ctx* ctx, int group, size_t n, const zk
   const int c0 = (int)default_window(n);
   std::vector<zkg_msm_tuning> out;
   for (int c = std::max(9, c0 - 2); c <= std::min(20, c0 + 2); c++) {
-    const uint32_t windows = (255 + c - 1) / c;
-    for (uint32_t L : {16u, 32u, 64u, 128u, 256u}) {
-      // keep at least a few waves of threads on 148 SMs
-      if ((double)n * windows / L < 148.0 * 256 && L > 16) continue;
-      std::unique_ptr<MsmPlan> plan;
-      try {
-        plan.reset(new MsmPlan(ctx, group, n, (uint32_t)c, L));
-      } catch (const Error& e) {
-        if (e.code == ZKG_ENOMEM) {
-          cudaGetLastError();
-          continue;
+    // G1 with c <= 16 also with the GLV split (2n points, ceil(128 / c) windows)
+    for (int glv = 0; glv <= (group == ZKG_G1 && c <= 16 ? 1 : 0); glv++) {
+      const uint32_t windows = glv ? (128 + c - 1) / c : (255 + c - 1) / c;
+      const double entries = (double)n * (glv ? 2 : 1) * windows;
+      for (uint32_t L : {16u, 32u, 64u, 128u, 256u}) {
+        // keep at least a few waves of threads on 148 SMs
+        if (entries / L < 148.0 * 256 && L > 16) continue;
+        std::unique_ptr<MsmPlan> plan;
+        try {
+          plan.reset(new MsmPlan(ctx, group, n, (uint32_t)c, L));
+          plan->set_glv(glv != 0);
+        } catch (const Error& e) {
+          if (e.code == ZKG_ENOMEM) {
+            cudaGetLastError();
+            continue;
+          }
+          throw;
         }
-        throw;
-      }
-      plan->check_buffers(bases, scalars);
-      // forms that can win: out-of-line integer products (1, 2) and, for G1, double-precision
-      // limbs (3, 4); fully inlined products (0) lose to both everywhere measured
-      const std::vector<int> variants = group == ZKG_G1 ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{1, 2};
-      for (int v : variants) {
-        plan->acc_variant = v;
-        double ms = time_ms(ctx->stream, reps, [&] { plan->enqueue(bases->ptr, scalars->ptr, ctx->stream); });
-        out.push_back(zkg_msm_tuning{(uint32_t)c, L, v, ms});
+        plan->check_buffers(bases, scalars);
+        // forms that can win: out-of-line integer products (1, 2) and, for G1, double-precision
+        // limbs (3, 4); fully inlined products (0) lose to both everywhere measured
+        const std::vector<int> variants = group == ZKG_G1 ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{1, 2};
+        for (int v : variants) {
+          plan->acc_variant = v;
+          double ms = time_ms(ctx->stream, reps, [&] { plan->enqueue(bases->ptr, scalars->ptr, ctx->stream); });
+          out.push_back(zkg_msm_tuning{(uint32_t)c, L, v, glv, ms});
+        }
       }
     }
   }

@@ -20,7 +20,7 @@ class StageTime(ctypes.Structure):
 
 class MsmTuning(ctypes.Structure):
     _fields_ = [("c", ctypes.c_uint32), ("item_points", ctypes.c_uint32), ("variant", ctypes.c_int),
-                ("ms", ctypes.c_double)]
+                ("glv", ctypes.c_int), ("ms", ctypes.c_double)]
 
 
 class ServerConfig(ctypes.Structure):

@@ -2,7 +2,7 @@
 module caches its choices on disk, keyed by (device name, operation, size, group), so a process
 pays for the search once per configuration.
 
-    msm = tuned_msm(gpu, Group.G1, n, bases, scalars)   # Msm with the fastest (c, L, form)
+    msm = tuned_msm(gpu, Group.G1, n, bases, scalars)   # Msm with the fastest (c, L, form, GLV)
     ntt = tuned_ntt(gpu, log_n, data)                   # Ntt with the fastest pass split
 
 Cache: $ZK_GPU_TUNE_CACHE, else ~/.cache/zk_gpu/autotune.json.
@@ -48,13 +48,13 @@ def search_msm(gpu: Gpu, group: Group, n: int, bases: Buffer, scalars: Buffer, r
     count = ctypes.c_size_t()
     check(lib().zkg_tune_msm(gpu.handle, int(group), n, bases.handle, scalars.handle, reps, arr, 128,
                              ctypes.byref(count)))
-    return [{"c": arr[i].c, "item_points": arr[i].item_points, "variant": arr[i].variant, "ms": arr[i].ms}
-            for i in range(count.value)]
+    return [{"c": arr[i].c, "item_points": arr[i].item_points, "variant": arr[i].variant, "glv": arr[i].glv,
+             "ms": arr[i].ms} for i in range(count.value)]
 
 
 def tuned_msm(gpu: Gpu, group: Group, n: int, bases: Buffer, scalars: Buffer, reps: int = 2,
               refresh: bool = False) -> Msm:
-    key = f"{gpu.adapter_name}|msm|{int(group)}|{n}"
+    key = f"{gpu.adapter_name}|msm2|{int(group)}|{n}"
     cache = _load()
     if refresh or key not in cache:
         best = search_msm(gpu, group, n, bases, scalars, reps)[0]
@@ -63,6 +63,7 @@ def tuned_msm(gpu: Gpu, group: Group, n: int, bases: Buffer, scalars: Buffer, re
     p = cache[key]
     msm = Msm.for_group(gpu, group, n, p["c"], p["item_points"])
     msm.set_variant(p["variant"])
+    msm.set_glv(bool(p.get("glv", 0)))
     return msm
 
 

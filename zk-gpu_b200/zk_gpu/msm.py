@@ -102,7 +102,8 @@ class Msm:
     def params(self) -> dict:
         c, items, var = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
         check(lib().zkg_msm_params(self._h, ctypes.byref(c), ctypes.byref(items), ctypes.byref(var)))
-        return {"c": c.value, "item_points": items.value, "variant": var.value}
+        windows, glv = self.windows()
+        return {"c": c.value, "item_points": items.value, "variant": var.value, "windows": windows, "glv": glv}
 
     def run(self, gpu: Gpu, bases: Buffer, scalars: Buffer) -> Buffer:
         """Msm::run: queue sum(scalars[i] * bases[i]); returns the plan's XYZZ result buffer
