@@ -18,14 +18,9 @@ struct BaseParams<Fp<P>> {
   using type = P;
 };
 
-// Scratch: 32 lanes x LaneWords<F> words in shared memory (8-byte aligned), owned by the warp.
+// Scratch: 32 lanes x 8 words in shared memory, owned by the warp.
 struct LaneScratch {
   uint32_t* words;
-};
-// Words one lane exchanges per product: one 8-word element (a base element for Fq2 products).
-template <class F>
-struct LaneWords {
-  static constexpr int value = 8;
 };
 
 template <class P>

@@ -15,7 +15,6 @@
 #include "msm.hpp"
 #include "msm_f64.cuh"
 #include "msm_kernels.cuh"
-#include "tail_f64.cuh"
 
 namespace zkg {
 
@@ -340,31 +339,18 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
-    case kStageCombine: {
+    case kStageCombine:
       // c (W - 1) dependent doublings: one warp, each level's independent products on separate
       // lanes (one out-of-line product per lane).
-      const uint32_t base = glv ? 128u / windows : c, extra = glv ? 128u % windows : 0u;
-      if constexpr (std::is_same<F, Fq>::value) {
-        if (tail_form == 1) {
-          msm_combine_lanes<FqT><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), base, extra, result.ptr);
-          check_launch("msm_combine_lanes");
-          break;
-        }
-      }
-      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), base, extra,
+      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
+                                                                       glv ? 128u / windows : c,
+                                                                       glv ? 128u % windows : 0u,
                                                                        result.ptr);
       check_launch("msm_combine_lanes");
       break;
-    }
     case kStageMerge:
     case kStageReduce:
     case kStageWindows:
-      if constexpr (std::is_same<F, Fq>::value) {
-        if (tail_form == 1) {
-          tail_stage<FqT>(which, s);
-          break;
-        }
-      }
       // Two products per out-of-line call in every form (measured faster than one per call for
       // both groups, although the paired Fq2 kernels spill).
       tail_stage<typename PairedOf<F>::type>(which, s);

@@ -816,7 +816,7 @@ __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t
   constexpr int XW = PointWords<F>::xyzz;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Xyzz<F>* sh = reinterpret_cast<Xyzz<F>*>(smem_raw);
-  __shared__ __align__(8) uint32_t scratch[32 * LaneWords<F>::value];
+  __shared__ uint32_t scratch[32 * 8];
   const LaneScratch sm{scratch};
   const uint32_t w = blockIdx.x;
   Xyzz<F> acc = xyzz_infinity<F>();
@@ -841,7 +841,7 @@ __global__ void __launch_bounds__(kWindowThreads) msm_window_sums(const uint32_t
 template <class F>
 __global__ void __launch_bounds__(32) msm_combine_lanes(const uint32_t* __restrict__ window_sums, uint32_t windows,
                                                         uint32_t base, uint32_t extra, uint32_t* __restrict__ result) {
-  __shared__ __align__(8) uint32_t scratch[32 * LaneWords<F>::value];
+  __shared__ uint32_t scratch[32 * 8];
   const LaneScratch sm{scratch};
   constexpr int XW = PointWords<F>::xyzz;
   Xyzz<F> acc = load_xyzz<F>(window_sums + (size_t)(windows - 1) * XW);
