@@ -74,7 +74,8 @@ def parse():
     ap.add_argument("--ntt-form", type=int, choices=[0, 1, 2, 3], default=None,
                     help="profiling case: NTT butterfly form (default: the plan's default)")
     ap.add_argument("--profile-parts", default="g1,ntt,g2,elementwise",
-                    help="profiling case: which parts run (g1, ntt, g2, elementwise), comma-separated")
+                    help="profiling case: which parts run (g1, g1_16, ntt, g2, elementwise), comma-separated; "
+                         "g1_16 is three runs of a G1 MSM 2^16")
     return ap.parse_args()
 
 
@@ -822,6 +823,8 @@ def profile_case(msm_form=None, ntt_form=None, parts="g1,ntt,g2,elementwise"):
         x = ctypes.c_double()
         check(lib().zkg_bench_integer_pipe(gpu.handle, 3, ctypes.byref(x)))
         profile_g1(gpu, msm_form)
+    if "g1_16" in parts:
+        profile_g1(gpu, msm_form, log_n=16, runs=3)
     if "ntt" in parts:
         profile_ntt(gpu, ntt_form)
     if "g2" in parts:
@@ -831,17 +834,18 @@ def profile_case(msm_form=None, ntt_form=None, parts="g1,ntt,g2,elementwise"):
     print("profile case done", flush=True)
 
 
-def profile_g1(gpu, msm_form):
+def profile_g1(gpu, msm_form, log_n=22, runs=1):
     from zk_gpu import Group, Msm
     from zk_gpu.synthetic import generator_multiples, uniform_scalars
 
-    n = 1 << 22
+    n = 1 << log_n
     bases = generator_multiples(gpu, Group.G1, uniform_scalars(n, 1), mont256=True)
     s = gpu.buffer(uniform_scalars(n, 2))
     msm = Msm(gpu, n, Msm.default_window(n))
     if msm_form is not None:
         msm.set_variant(msm_form)
-    msm.run(gpu, bases, s)
+    for _ in range(runs):
+        msm.run(gpu, bases, s)
     gpu.wait()
     msm.close()
     bases.free()
