@@ -137,6 +137,10 @@ int zkg_msm_set_sort(zkg_msm *msm, int mode);
  * window, so the stores of one window meet in L2 (default; applies for c <= 16, larger c use 0;
  * 6 more bytes of plan memory per (window, point) entry). */
 int zkg_msm_set_sort_form(zkg_msm *msm, int form);
+/* Tail-stage form (no reference counterpart; G1, G2 ignores it): the merge levels, running-sum
+ * reductions, window sums and Horner combination compute with 0 = 32-bit integer Montgomery
+ * products two per out-of-line call (default), 1 = the products inlined. */
+int zkg_msm_set_tail_form(zkg_msm *msm, int form);
 /* Fixed-base MSM over a resident key (no reference counterpart: the reference combines its
  * windows by Horner, msm_combine.wgsl:13-22, on every run). zkg_msm_fixed_base_table builds, once
  * per key and window size c, a table of ceil(255/c) rows of n points, row w holding 2^(c w) P_i

@@ -342,15 +342,23 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
     case kStageCombine:
       // c (W - 1) dependent doublings: one warp, each level's independent products on separate
       // lanes (one out-of-line product per lane).
-      msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
-                                                                       glv ? 128u / windows : c,
-                                                                       glv ? 128u % windows : 0u,
-                                                                       result.ptr);
+      if (std::is_same<F, Fq>::value && tail_form == 1)
+        msm_combine_lanes<Fq><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), glv ? 128u / windows : c,
+                                               glv ? 128u % windows : 0u, result.ptr);
+      else
+        msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
+                                                                         glv ? 128u / windows : c,
+                                                                         glv ? 128u % windows : 0u,
+                                                                         result.ptr);
       check_launch("msm_combine_lanes");
       break;
     case kStageMerge:
     case kStageReduce:
     case kStageWindows:
+      if (std::is_same<F, Fq>::value && tail_form == 1) {
+        tail_stage<Fq>(which, s);
+        break;
+      }
       // Two products per out-of-line call in every form (measured faster than one per call for
       // both groups, although the paired Fq2 kernels spill).
       tail_stage<typename PairedOf<F>::type>(which, s);

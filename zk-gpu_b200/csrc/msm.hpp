@@ -52,6 +52,9 @@ struct MsmPlan {
   // pass records each digit's rank in its slot, the placing pass runs window by window;
   // msm_rank / msm_place). 1 is the default where it applies (c <= 16).
   int sort_form = 1;
+  // Tail stages (merge, reductions, window sums, combination) of G1: 0 = integer products two
+  // per out-of-line call, 1 = products inlined (the independent products of a level interleave).
+  int tail_form = 0;
   bool ranked_sort() const { return fixed_base || glv || (sort_form == 1 && c <= 16); }
   // Fixed-base mode: `bases` of run() is a table from fixed_base_table() (windows * n points,
   // row w = 2^(c w) P_i), every window's digits share one set of 2^(c-1) buckets, and the
