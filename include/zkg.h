@@ -137,10 +137,6 @@ int zkg_msm_set_sort(zkg_msm *msm, int mode);
  * window, so the stores of one window meet in L2 (default; applies for c <= 16, larger c use 0;
  * 6 more bytes of plan memory per (window, point) entry). */
 int zkg_msm_set_sort_form(zkg_msm *msm, int form);
-/* Tail-stage form (no reference counterpart; G1, G2 ignores it): the merge levels, running-sum
- * reductions, window sums and Horner combination compute with 0 = 32-bit integer Montgomery
- * products two per out-of-line call (default), 1 = the products inlined. */
-int zkg_msm_set_tail_form(zkg_msm *msm, int form);
 /* Fixed-base MSM over a resident key (no reference counterpart: the reference combines its
  * windows by Horner, msm_combine.wgsl:13-22, on every run). zkg_msm_fixed_base_table builds, once
  * per key and window size c, a table of ceil(255/c) rows of n points, row w holding 2^(c w) P_i
@@ -155,7 +151,7 @@ int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
 /* GLV splitting for G1 (no reference counterpart; the reference names GLV as a next step,
  * README.md:223-224): with enable = 1 every scalar k is split as k1 + k2 lambda (mod r), |k1|,
  * |k2| < 2^127, and a run sums k1_i P_i + k2_i phi(P_i) with phi(x, y) = (beta x, y): 2n points
- * (the plan makes +-phi(P_i) from `bases` on every run, 128 more bytes of plan memory per point)
+ * (the plan makes phi(P_i) from `bases` on every run, 64 more bytes of plan memory per point)
  * with W = ceil(128 / c) windows instead of ceil(255 / c), the 128 bits spread over them as
  * evenly as possible (widths floor(128 / W) or one more, never above c), so about the same number
  * of bucket additions and half the bucket reductions and combination doublings. The result is the same point as the

@@ -43,11 +43,10 @@ def msm_ref(group: str, bases: np.ndarray, scalars: np.ndarray, mont256: bool = 
 
 
 def gpu_msm(gpu, bases: np.ndarray, scalars: np.ndarray, plan=None, group: Group = Group.G1,
-            variant=None, glv=None, tail_form=None) -> np.ndarray:
+            variant=None, glv=None) -> np.ndarray:
     """Upload plain bases and scalars, run one MSM and return the affine result words
     (zeros = infinity). plan = None uses the defaults; (c, item_points) overrides them;
-    variant selects the accumulation kernel's form; glv switches the G1 GLV split on or off;
-    tail_form selects the tail stages' product form."""
+    variant selects the accumulation kernel's form; glv switches the G1 GLV split on or off."""
     n = scalars.size // 8
     base_buf = Msm.upload_bases(gpu, bases)
     scalar_buf = gpu.buffer(scalars)
@@ -59,8 +58,6 @@ def gpu_msm(gpu, bases: np.ndarray, scalars: np.ndarray, plan=None, group: Group
         msm.set_variant(variant)
     if glv is not None:
         msm.set_glv(glv)
-    if tail_form is not None:
-        msm.set_tail_form(tail_form)
     out = msm.run(gpu, base_buf, scalar_buf)
     words = gpu.read(out, group.xyzz_words())
     if group == Group.G1:

@@ -70,8 +70,6 @@ def test_tuning_knobs_reject_out_of_range_values(gpu):
         g2.set_variant(-1)
     assert g2.params()["variant"] == 2 and g1.params()["variant"] == 3
     assert Msm(gpu, 1 << 23, 16).params()["variant"] == 4  # 2^27 entries: one product per call
-    with pytest.raises(ZkGpuError, match="tail form must be 0 or 1"):
-        g1.set_tail_form(2)
     ntt = Ntt(gpu, 12)
     with pytest.raises(ZkGpuError, match="NTT variant must be 0..4"):
         ntt.set_variant(5)

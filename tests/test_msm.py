@@ -17,13 +17,13 @@ R = bn254.R
 
 
 def check(gpu, bases, scalars, c, what, variant=None):
-    """Both the plain windows and the default (the GLV split for G1, c <= 16), and both tail
-    forms (products two per out-of-line call, and inlined)."""
+    """Both the plain windows and the default (the GLV split for G1, c <= 16)."""
     expected = msm_ref("G1", bases, scalars)
-    for item_points, glv, tail in ((1024, False, 0), (1024, None, 1), (7, False, 1), (7, None, 0)):
-        got = gpu_msm(gpu, bases, scalars, (c, item_points), variant=variant, glv=glv, tail_form=tail)
-        assert np.array_equal(got, expected), (f"{what} (n = {scalars.size // 8}, c = {c}, item_points = "
-                                               f"{item_points}, variant = {variant}, glv = {glv}, tail = {tail})")
+    for item_points in (1024, 7):
+        for glv in (False, None):
+            got = gpu_msm(gpu, bases, scalars, (c, item_points), variant=variant, glv=glv)
+            assert np.array_equal(got, expected), (f"{what} (n = {scalars.size // 8}, c = {c}, item_points = "
+                                                   f"{item_points}, variant = {variant}, glv = {glv})")
 
 
 # Accumulation kernel forms checked by the edge-case suites: the default, and the G1 forms
@@ -238,11 +238,11 @@ def fuzz_case(gpu, seed):
     else:
         s = fr_words([0, 1, R - 1][int(v)] for v in rnd.integers(0, 3, size=n))
     bases = np.ascontiguousarray(bases.reshape(-1))
-    glv, tail = bool(rnd.integers(0, 2)), int(rnd.integers(0, 2))
-    got = gpu_msm(gpu, bases, s, (c, item_points), glv=glv, tail_form=tail)
+    glv = bool(rnd.integers(0, 2))
+    got = gpu_msm(gpu, bases, s, (c, item_points), glv=glv)
     assert np.array_equal(got, msm_ref("G1", bases, s)), (
         f"FUZZ FAILURE: rerun with ZK_GPU_FUZZ_SEED={seed} (n={n}, c={c}, item_points={item_points}, "
-        f"scalars={scalar_kind}, bases={base_kind}, glv={glv}, tail={tail})")
+        f"scalars={scalar_kind}, bases={base_kind}, glv={glv})")
 
 
 def fuzz_forms_case(gpu, seed):
@@ -295,8 +295,7 @@ def test_fuzz(gpu):
 
 # ---------------------------------------------------------------- full sizes
 
-def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False, glv=None,
-                   tail_form=None):
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False, glv=None):
     """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
     uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G. tuned: the plan
     (window, points per thread, form) comes from the autotuner on these inputs."""
@@ -320,8 +319,6 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant
             msm.set_variant(variant)
         if glv is not None:
             msm.set_glv(glv)
-        if tail_form is not None:
-            msm.set_tail_form(tail_form)
     got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, scalar_buf), 32)))
     gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
     want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
@@ -348,13 +345,6 @@ def test_full_size_autotuned(gpu, log_n, kind, tmp_path, monkeypatch):
     """The same cases with the autotuned window, points per thread and form."""
     monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
     full_size_case(gpu, log_n, kind, tuned=True)
-
-
-@pytest.mark.parametrize("log_n", [18, 22])
-def test_full_size_tail_forms(gpu, log_n):
-    """The inlined-product tail stages at full size, with and without the GLV split."""
-    for glv in (False, True):
-        full_size_case(gpu, log_n, "r-1", glv=glv, tail_form=1)
 
 
 def test_full_size_other_window(gpu):

@@ -429,14 +429,6 @@ int zkg_msm_set_fixed_base(zkg_msm* msm, int enable) {
   });
 }
 
-int zkg_msm_set_tail_form(zkg_msm* msm, int form) {
-  return guard([&] {
-    need(msm, "msm");
-    if (form < 0 || form > 1) fail(ZKG_EINVAL, "tail form must be 0 or 1");
-    msm->plan.tail_form = form;
-  });
-}
-
 int zkg_msm_set_glv(zkg_msm* msm, int enable) {
   return guard([&] {
     need(msm, "msm");

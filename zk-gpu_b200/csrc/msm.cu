@@ -168,7 +168,7 @@ void MsmPlan::layout() {
   runs[0].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   runs[1].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   window_sums.alloc((size_t)windows * xw, "msm window sums");
-  if (glv) glv_bases.alloc(np * affine_words(), "msm GLV bases");
+  if (glv) glv_bases.alloc(n * affine_words(), "msm GLV bases (phi)");
   else glv_bases.release();
 }
 
@@ -246,13 +246,15 @@ void fixed_base_table(zkg_ctx* ctx, int group, const zkg_buf* bases, size_t n, u
 template <int AGG>
 void MsmPlan::rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
   const unsigned b256 = 256;
-  if (glv)
+  if (glv) {
+    msm_glv_phi<<<grid_for(n, b256), b256, 0, s>>>(bases, n, glv_bases.ptr);
+    check_launch("msm_glv_phi");
     msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), n, c, windows, 0, counts.ptr,
-                                                                   digits.as<uint16_t>(), ranks.ptr, bases,
-                                                                   glv_bases.ptr);
-  else
+                                                                   digits.as<uint16_t>(), ranks.ptr);
+  } else {
     msm_rank<AGG, false><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, n, c, windows, fixed_base, counts.ptr,
-                                                             digits.as<uint16_t>(), ranks.ptr, nullptr, nullptr);
+                                                             digits.as<uint16_t>(), ranks.ptr);
+  }
 }
 
 template <class F>
@@ -306,61 +308,61 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       msm_scatter<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
       check_launch("msm_scatter");
       break;
-    case kStageAccumulate:
-      if (glv) bases = glv_bases.ptr;
+    case kStageAccumulate: {
+      // GLV: points n..2n-1 are the phi(P_i) of glv_bases
+      const uint32_t* bases2 = glv ? glv_bases.ptr : bases;
+      const uint32_t split = glv ? (uint32_t)n : 0xffffffffu;
       if ((acc_variant == 5 || acc_variant == 6) && std::is_same<F, Fq>::value) {
         // G1 with the accumulator in shared memory, four blocks per SM
         const size_t acc_smem = f64_acc_smem<f64::FqD>(true);
         if (acc_variant == 5)
           msm_accumulate_f64<f64::FqD, false, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else
           msm_accumulate_f64<f64::FqD, true, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       } else if (acc_variant >= 3) {
         using E = typename std::conditional<std::is_same<F, Fq>::value, f64::FqD, f64::Fq2D>::type;
         const size_t acc_smem = f64_acc_smem<E>();
         if (acc_variant == 3 || acc_variant == 6)
           msm_accumulate_f64<E, true><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
         else
           msm_accumulate_f64<E, false><<<grid_for(heads_max, 128), 128, acc_smem, s>>>(
-              bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+              bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       }
       else if (acc_variant == 1)
         msm_accumulate<typename CompactOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+            bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else if (acc_variant == 2)
         msm_accumulate<typename PairedOf<F>::type><<<grid_for(heads_max, 128), 128, 0, s>>>(
-            bases, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
+            bases, bases2, split, sorted.ptr, slot_start.ptr, (uint32_t)active_slots(), seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       else
-        msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, sorted.ptr, slot_start.ptr,
+        msm_accumulate<F><<<grid_for(heads_max, 128), 128, 0, s>>>(bases, bases2, split, sorted.ptr, slot_start.ptr,
                                                                    (uint32_t)active_slots(),
                                                                    seg_len, buckets.ptr, heads[0].ptr, head_keys[0].ptr);
       check_launch("msm_accumulate");
       break;
+    }
     case kStageCombine:
       // c (W - 1) dependent doublings: one warp, each level's independent products on separate
-      // lanes (one out-of-line product per lane).
-      if (std::is_same<F, Fq>::value && tail_form == 1)
+      // lanes. G1 inlines its products (measured 5-8% faster than one out-of-line product per
+      // lane: 2^16 with GLV 0.287 -> 0.265 ms); G2 keeps the out-of-line Fq2 products.
+      if constexpr (std::is_same<F, Fq>::value)
         msm_combine_lanes<Fq><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), glv ? 128u / windows : c,
                                                glv ? 128u % windows : 0u, result.ptr);
       else
         msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
                                                                          glv ? 128u / windows : c,
-                                                                         glv ? 128u % windows : 0u,
-                                                                         result.ptr);
+                                                                         glv ? 128u % windows : 0u, result.ptr);
       check_launch("msm_combine_lanes");
       break;
     case kStageMerge:
     case kStageReduce:
     case kStageWindows:
-      if (std::is_same<F, Fq>::value && tail_form == 1) {
-        tail_stage<Fq>(which, s);
-        break;
-      }
       // Two products per out-of-line call in every form (measured faster than one per call for
-      // both groups, although the paired Fq2 kernels spill).
+      // both groups, although the paired Fq2 kernels spill, and than inlined products for G1:
+      // 2^24 merge 1.10 -> 1.49 ms, reduce 0.66 -> 1.09 ms inlined).
       tail_stage<typename PairedOf<F>::type>(which, s);
       break;
   }

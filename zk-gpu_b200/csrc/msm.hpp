@@ -52,9 +52,6 @@ struct MsmPlan {
   // pass records each digit's rank in its slot, the placing pass runs window by window;
   // msm_rank / msm_place). 1 is the default where it applies (c <= 16).
   int sort_form = 1;
-  // Tail stages (merge, reductions, window sums, combination) of G1: 0 = integer products two
-  // per out-of-line call, 1 = products inlined (the independent products of a level interleave).
-  int tail_form = 0;
   bool ranked_sort() const { return fixed_base || glv || (sort_form == 1 && c <= 16); }
   // Fixed-base mode: `bases` of run() is a table from fixed_base_table() (windows * n points,
   // row w = 2^(c w) P_i), every window's digits share one set of 2^(c-1) buckets, and the
@@ -62,12 +59,11 @@ struct MsmPlan {
   // Needs c <= 16 (the ranked sort).
   bool fixed_base = false;
   // GLV mode (G1, c <= 16): every scalar splits as k1 + k2 lambda with 127-bit halves, and the
-  // MSM runs over the 2n points +-P_i, +-phi(P_i) (glv_bases, made from `bases` on every run) with
+  // MSM runs over the 2n points P_i, phi(P_i) (phi(P_i) in glv_bases, made from `bases` on every
+  // run; each half-scalar's sign in its digits) with
   // W = ceil(128 / c) windows of floor(128 / W) or floor(128 / W) + 1 bits (glv_window_width):
   // about the same number of bucket additions, half the windows, so half the reductions and half
-  // the combination doublings. The counting pass writes glv_bases, each
-  // base carrying its half-scalar's sign: the digits' 16-bit codes (kRankZero) have no room for
-  // a sign flip at c = 16.
+  // the combination doublings.
   // On by default where it applies (glv_default); zkg_msm_set_glv switches it; fixed-base mode
   // switches it off.
   bool glv = false;
@@ -82,7 +78,7 @@ struct MsmPlan {
 
   DeviceArray counts, slot_start, cursor, tile_sums, sorted, buckets;
   DeviceArray ranks, digits;  // the ranked sort's rank (32 bits) and digit (16 bits) per (window, point), window-major
-  DeviceArray glv_bases;      // GLV mode: P_0..P_{n-1}, phi(P_0)..phi(P_{n-1})
+  DeviceArray glv_bases;      // GLV mode: phi(P_0)..phi(P_{n-1})
   DeviceArray heads[2], head_keys[2];
   DeviceArray tots, runs[2], window_sums, result;
   zkg_buf result_handle;

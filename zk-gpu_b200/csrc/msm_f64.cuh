@@ -297,7 +297,8 @@ __device__ __forceinline__ bool xyzzd_add_affine(Acc& acc, const E& bx, const E&
 // which frees its 40 registers for a fourth block per SM (128 registers).
 template <class E, bool PAIRS, bool SMEM_ACC = !std::is_same<E, f64::FqD>::value>
 __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? (SMEM_ACC ? 4 : 3) : 2)
-    msm_accumulate_f64(const uint32_t* __restrict__ bases, const uint32_t* __restrict__ sorted,
+    msm_accumulate_f64(const uint32_t* __restrict__ bases, const uint32_t* __restrict__ bases2, uint32_t split,
+                       const uint32_t* __restrict__ sorted,
                        const uint32_t* __restrict__ slot_start, uint32_t num_slots, uint32_t seg_len,
                        uint32_t* __restrict__ buckets, uint32_t* __restrict__ heads,
                        uint32_t* __restrict__ head_keys) {
@@ -325,8 +326,10 @@ __global__ void __launch_bounds__(128, std::is_same<E, f64::FqD>::value ? (SMEM_
   if constexpr (SMEM_ACC) acc.base = acc_slots + threadIdx.x;
   bool empty = true;
   __shared__ __align__(16) uint32_t stage[2][128][AW];
-  auto stage_base = [&](uint32_t slot, uint32_t e) {  // x then y
-    const uint4* g = reinterpret_cast<const uint4*>(bases + (size_t)(e & ~kNegBit) * AW);
+  auto stage_base = [&](uint32_t slot, uint32_t e) {  // x then y; points from split on in bases2
+    const uint32_t pt = e & ~kNegBit;
+    const uint4* g = reinterpret_cast<const uint4*>(pt < split ? bases + (size_t)pt * AW
+                                                               : bases2 + (size_t)(pt - split) * AW);
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(&stage[slot][threadIdx.x][0]);
 #pragma unroll
     for (int k = 0; k < AW / 4; k++)

@@ -77,17 +77,25 @@ struct Recoder {
     }
     return mag ? w * half + mag - 1 : kNoKey;
   }
-  // The same for a window of `width` bits starting at bit `pos` (width <= c: the GLV windows).
-  __device__ __forceinline__ uint32_t next_at(uint32_t w, uint32_t pos, uint32_t width, uint32_t half, bool* neg) {
-    uint32_t v = window_bits(s, pos, width) + carry;
+  // The same for a window of `width` bits starting at bit `pos` (width <= c: the GLV windows),
+  // the digit negated when `flip` (a negative half-scalar: its digits are those of |k| with the
+  // sign turned). A flipped half is recoded with v > 2^(width-1) negative instead of >=, so its
+  // digits lie in (-2^(width-1), 2^(width-1)] and, turned, in [-2^(width-1), 2^(width-1)) like
+  // every other digit: the positive magnitude 2^(c-1), whose 16-bit code is kRankZero at c = 16,
+  // never occurs.
+  __device__ __forceinline__ uint32_t next_at(uint32_t w, uint32_t pos, uint32_t width, uint32_t half, bool flip,
+                                              bool* neg) {
+    const uint32_t v = window_bits(s, pos, width) + carry;
+    const uint32_t h = 1u << (width - 1);
     carry = 0;
     uint32_t mag = v;
-    *neg = false;
-    if (v >= (1u << (width - 1))) {
+    bool neg_d = false;
+    if (flip ? v > h : v >= h) {
       mag = (1u << width) - v;
-      *neg = true;
+      neg_d = true;
       carry = 1;
     }
+    *neg = neg_d != flip;
     return mag ? w * half + mag - 1 : kNoKey;
   }
 };
@@ -334,21 +342,20 @@ __device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
 }
 }  // namespace glv
 
-// Base of GLV entry i (point src = i mod n; second: the k2 half): P_src or phi(P_src) = (beta x,
-// y), negated ((x, q - y)) when that half of the scalar is negative, so the digits keep their own
-// signs. Affine, Montgomery form; infinity, (0, 0), stays (0, 0).
-__device__ __forceinline__ void glv_base(const uint32_t* __restrict__ bases, size_t src, bool second, bool neg,
-                                         uint32_t* __restrict__ out) {
-  Fq x = load_fe<Fq>(bases + 16 * src), y = load_fe<Fq>(bases + 16 * src + 8);
-  if (second) {
-    Fq beta;
+// phi(P_i) = (beta x_i, y_i) for the n bases (affine, Montgomery form; infinity, (0, 0), stays
+// (0, 0)): the bases of GLV entries n..2n-1. Entries 0..n-1 read P_i from the caller's bases, and
+// every entry's half-scalar sign is in its digits.
+__global__ void msm_glv_phi(const uint32_t* __restrict__ bases, size_t n, uint32_t* __restrict__ phi) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Fq beta;
 #pragma unroll
-    for (int k = 0; k < 8; k++) beta.w[k] = glv::kBetaMont[k];
-    x = x * beta;
-  }
-  if (neg && !y.is_zero()) y = Fq::zero() - y;
-  store_fe(out, x);
-  store_fe(out + 8, y);
+  for (int k = 0; k < 8; k++) beta.w[k] = glv::kBetaMont[k];
+  const uint4* src = reinterpret_cast<const uint4*>(bases + 16 * i);
+  store_fe(phi + 16 * i, load_fe<Fq>(bases + 16 * i) * beta);
+  uint4* dst = reinterpret_cast<uint4*>(phi + 16 * i);
+  dst[2] = __ldg(src + 2);
+  dst[3] = __ldg(src + 3);
 }
 
 // ------------------------------------------------------------------ ranked counting sort
@@ -367,24 +374,22 @@ constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occ
 
 // fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
 // window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
-// GLV: n = 2 scalar_n points; entry i < scalar_n takes |k1| of scalar i, entry scalar_n + i
-// takes |k2| of scalar i (glv::split_half), and glv_bases[i] gets the matching base with that
-// half's sign (glv_base).
+// GLV: n = 2 scalar_n points; entry i < scalar_n takes |k1| of scalar i (base P_i), entry
+// scalar_n + i takes |k2| of scalar i (base phi(P_i)), each with its half's sign folded into its
+// digits (glv::split_half, Recoder::next_at).
 template <int AGG, bool GLV = false>
 __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t scalar_n, uint32_t c, uint32_t windows,
                          int fixed, uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
-                         uint32_t* __restrict__ ranks, const uint32_t* __restrict__ bases,
-                         uint32_t* __restrict__ glv_bases) {
+                         uint32_t* __restrict__ ranks) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
   Recoder rc;
+  bool flip = false;
   if (live) {
     if (GLV) {
       const bool second = i >= scalar_n;
-      const size_t src = second ? i - scalar_n : i;
-      load_scalar(scalars, src, rc.s);
-      const bool neg = glv::split_half(rc.s, second);
-      glv_base(bases, src, second, neg, glv_bases + 16 * i);
+      load_scalar(scalars, second ? i - scalar_n : i, rc.s);
+      flip = glv::split_half(rc.s, second);
     } else {
       load_scalar(scalars, i, rc.s);
     }
@@ -405,7 +410,7 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t 
       neg[k] = false;
       if (w < windows) {  // uniform across the warp
         if (live)
-          slot[k] = GLV ? rc.next_at(w, glv_window_pos(w, windows), glv_window_width(w, windows), half, &neg[k])
+          slot[k] = GLV ? rc.next_at(w, glv_window_pos(w, windows), glv_window_width(w, windows), half, flip, &neg[k])
                         : rc.next(w, c, half, &neg[k]);
         if (fixed && slot[k] != kNoKey) slot[k] -= w * half;
         peers[k] = slot_peers<AGG>(slot[k]);
@@ -579,8 +584,11 @@ __device__ __forceinline__ Affine<F> load_signed_base(const uint32_t* __restrict
 
 // One thread per segment [t*L, t*L + L) of the sorted entries (all windows concatenated, slot
 // order). slot_start has num_slots + 1 entries; slot_start[num_slots] = total entries.
+// Points below `split` come from `bases`, the others from bases2 (point - split): the GLV
+// entries' P_i and phi(P_i); plain plans pass split = 2^32 - 1.
 template <class F>
 __global__ void __launch_bounds__(128) msm_accumulate(const uint32_t* __restrict__ bases,
+                                                      const uint32_t* __restrict__ bases2, uint32_t split,
                                                       const uint32_t* __restrict__ sorted,
                                                       const uint32_t* __restrict__ slot_start, uint32_t num_slots,
                                                       uint32_t seg_len, uint32_t* __restrict__ buckets,
@@ -606,7 +614,9 @@ __global__ void __launch_bounds__(128) msm_accumulate(const uint32_t* __restrict
   constexpr int AW = PointWords<F>::affine;  // 16 (G1) or 32 (G2) words
   __shared__ __align__(16) uint32_t stage[2][128][AW];
   auto stage_base = [&](uint32_t slot, uint32_t e) {
-    const uint4* g = reinterpret_cast<const uint4*>(bases + (size_t)(e & ~kNegBit) * AW);
+    const uint32_t pt = e & ~kNegBit;
+    const uint4* g = reinterpret_cast<const uint4*>(pt < split ? bases + (size_t)pt * AW
+                                                               : bases2 + (size_t)(pt - split) * AW);
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(&stage[slot][threadIdx.x][0]);
 #pragma unroll
     for (int k = 0; k < AW / 4; k++)

@@ -121,9 +121,9 @@ size_t Server::estimate_bytes(uint32_t log_m) const {
     const size_t entries = std::max((size_t)W * m, glv ? (size_t)Wg * 2 * m : 0), L = 8;  // worst-case segment
     const size_t heads = entries / L + 1;
     // counts, slot starts, cursors; sorted entries, ranks and digits; buckets; heads; running
-    // sums; the GLV bases (2m affine points)
+    // sums; the GLV bases (phi of the m points)
     return 4 * (3 * S + entries * 5 / 2 + S * xw + (heads + heads / 16 + 2) * (xw + 1) + 8 * W * B / 16 * xw / 8 +
-                (glv ? 2 * m * 16 : 0) + 4096);
+                (glv ? m * 16 : 0) + 4096);
   };
   // scratch, twiddle words (both directions), staged twiddle tables (both directions: 40 bytes
   // per element for the first pass, at most as much again for the later passes' small tables

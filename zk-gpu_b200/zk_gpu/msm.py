@@ -83,10 +83,6 @@ class Msm:
         check(lib().zkg_msm_fixed_base_table(gpu.handle, int(group), bases.handle, n, c, ctypes.byref(h)))
         return Buffer(gpu, h.value)
 
-    def set_tail_form(self, form: int) -> None:
-        """Tail stages of G1: 0 integer products two per out-of-line call, 1 inlined."""
-        check(lib().zkg_msm_set_tail_form(self._h, form))
-
     def set_glv(self, enable: bool = True) -> None:
         """G1: split every scalar as k1 + k2 lambda (mod r) and run over P_i and phi(P_i) with
         ceil(128 / c) windows; the same result as the plain MSM."""
