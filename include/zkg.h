@@ -162,6 +162,17 @@ int zkg_msm_set_fixed_base(zkg_msm *msm, int enable);
  * whether GLV is on. */
 int zkg_msm_set_glv(zkg_msm *msm, int enable);
 int zkg_msm_windows(const zkg_msm *msm, uint32_t *windows, int *glv);
+/* Runs in passes (no reference counterpart; the reference sizes one pass for n < 2^31,
+ * src/shaders/msm_digits.wgsl:33). Entry positions and point indices are 32-bit, so one pass holds
+ * fewer than 2^32 (window, point) entries (about 2^28 points at c = 16); a plan over more points
+ * runs over consecutive slices of at most `chunk` points and adds their results, so every n <
+ * 2^31 works. The plan's scratch is sized for one slice: zkg_msm_set_chunk(msm, points) sets a
+ * smaller slice to bound the plan's device memory (0 restores the largest; values above it are
+ * clamped; re-sizes the scratch, synchronising with queued work). A fixed-base plan runs in one
+ * pass (ZKG_EINVAL). zkg_msm_passes reports the slice and the number of passes. The result is
+ * the same point for every slice size. */
+int zkg_msm_set_chunk(zkg_msm *msm, size_t points);
+int zkg_msm_passes(const zkg_msm *msm, size_t *chunk, size_t *passes);
 int zkg_msm_params(const zkg_msm *msm, uint32_t *c, uint32_t *item_points, int *variant);
 /* Msm::run (src/msm.rs:284-298): queue sum(scalars[i] * bases[i]); scalars are 8 plain u32
  * words each. *result is a borrowed handle to the plan's XYZZ result (32 words G1, 64 words G2,

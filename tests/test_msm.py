@@ -295,7 +295,8 @@ def test_fuzz(gpu):
 
 # ---------------------------------------------------------------- full sizes
 
-def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False, glv=None):
+def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant=None, tuned=False, glv=None,
+                   chunk=None):
     """Bases [k_i]G built on the device (0.1% at infinity: k_i = 0), read back in plain form and
     uploaded through Msm::upload_bases; the expected result is [sum_i s_i k_i]G. tuned: the plan
     (window, points per thread, form) comes from the autotuner on these inputs."""
@@ -319,6 +320,8 @@ def full_size_case(gpu, log_n, kind, c=None, inf_fraction=0.001, seed=0, variant
             msm.set_variant(variant)
         if glv is not None:
             msm.set_glv(glv)
+        if chunk is not None:
+            msm.set_chunk(chunk)
     got = affine_words(xyzz_to_affine(gpu.read(msm.run(gpu, base_buf, scalar_buf), 32)))
     gen = np.array(bn254.affine_words("G1", bn254.G1_GEN), dtype=np.uint32)
     want = cpu.scalar_mul("G1", gen, cpu.fr_dot(s, k))
@@ -345,6 +348,12 @@ def test_full_size_autotuned(gpu, log_n, kind, tmp_path, monkeypatch):
     """The same cases with the autotuned window, points per thread and form."""
     monkeypatch.setenv("ZK_GPU_TUNE_CACHE", str(tmp_path / "tune.json"))
     full_size_case(gpu, log_n, kind, tuned=True)
+
+
+def test_full_size_in_passes(gpu):
+    """A 2^22 run in passes of 2^20 and of 3 x 10^5 points (a short last pass), GLV and plain."""
+    full_size_case(gpu, 22, "uniform", chunk=1 << 20)
+    full_size_case(gpu, 22, "r-1", glv=False, chunk=300000)
 
 
 def test_full_size_other_window(gpu):
@@ -470,3 +479,43 @@ def test_fixed_base_checks(gpu):
     msm.set_fixed_base(True)
     with pytest.raises(Exception, match="bases buffer holds"):
         msm.run(gpu, bases, gpu.buffer(random_fr(986, n)))  # the key itself, not its table
+
+
+@pytest.mark.parametrize("group", ["G1", "G2"])
+def test_passes(gpu, group):
+    """Runs split into passes of at most `chunk` points (zkg_msm_set_chunk) give the one-pass
+    point for every slice size, including one point per pass and a short last pass; the plan's
+    stage profile sums the passes; a fixed-base plan runs in one pass."""
+    grp = Group.G1 if group == "G1" else Group.G2
+    n = 5000 if group == "G1" else 1200
+    bases = random_points(group, 1900, n)
+    bases[: grp.affine_words() * 2] = 0  # two points at infinity
+    s = random_fr(1901, n).reshape(n, 8)
+    s[5] = bn254.words32(R - 1)
+    s[6] = 0
+    s = s.reshape(-1)
+    want = msm_ref(group, bases, s)
+    base_buf, scalar_buf = Msm.upload_bases(gpu, bases), gpu.buffer(s)
+    conv = xyzz_to_affine if grp == Group.G1 else xyzz_to_affine_g2
+    chunks = [1, 7, 1000, n // 2, n - 1, n, 10 * n, 0] if group == "G1" else [333, n - 1, 0]
+    for glv in ((False, True) if group == "G1" else (False,)):
+        msm = Msm.for_group(gpu, grp, n, 11)
+        msm.set_glv(glv)
+        assert msm.passes() == (n, 1)
+        for ch in chunks:
+            msm.set_chunk(ch)
+            per = min(ch or n, n)
+            assert msm.passes() == (per, -(-n // per)), (ch, msm.passes())
+            for _ in range(2):  # the scratch of every pass is reused
+                got = affine_words(conv(gpu.read(msm.run(gpu, base_buf, scalar_buf), grp.xyzz_words())), grp)
+                assert np.array_equal(got, want), (group, glv, ch)
+    msm = Msm.for_group(gpu, grp, n, 11)
+    msm.set_chunk(1000)
+    stages = msm.profile(gpu, base_buf, scalar_buf)
+    assert len(stages) == 8 and all(ms >= 0 for _, ms in stages)
+    got = affine_words(conv(gpu.read(msm.run(gpu, base_buf, scalar_buf), grp.xyzz_words())), grp)
+    assert np.array_equal(got, want)
+    msm.set_fixed_base(True)  # one pass: the table's rows are n points apart
+    assert msm.passes() == (n, 1)
+    with pytest.raises(Exception, match="runs in one pass"):
+        msm.set_chunk(100)

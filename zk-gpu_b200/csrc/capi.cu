@@ -436,6 +436,21 @@ int zkg_msm_set_glv(zkg_msm* msm, int enable) {
   });
 }
 
+int zkg_msm_set_chunk(zkg_msm* msm, size_t points) {
+  return guard([&] {
+    need(msm, "msm");
+    msm->plan.set_chunk(points);
+  });
+}
+
+int zkg_msm_passes(const zkg_msm* msm, size_t* chunk, size_t* passes) {
+  return guard([&] {
+    need(msm, "msm");
+    if (chunk) *chunk = msm->plan.chunk;
+    if (passes) *passes = msm->plan.passes();
+  });
+}
+
 int zkg_msm_windows(const zkg_msm* msm, uint32_t* windows, int* glv) {
   return guard([&] {
     need(msm, "msm");

@@ -55,13 +55,13 @@ uint32_t default_window(size_t n) {
 }
 
 // Points accumulated per thread when the caller does not choose, by the number of (point,
-// window) entries; measured on B200 (G1, uniform scalars, sweeping 8..128): 2^14 points best at
-// 8, 2^16 at 16, 2^18 at 32, 2^20 at 64, 2^22 and 2^24 at 128 (longer segments lengthen the
-// accumulation chains, shorter ones add heads and merge levels).
+// window) entries; measured on B200 (G1, uniform scalars, default windows with the GLV split,
+// sweeping 8..256): 2^16 points (1.6M entries) best at 32 (1.26 ms against 1.34 at 16: fewer
+// merge levels), 2^18 at 32, 2^20 at 64-128, 2^22 and 2^24 at 128; 2^14 at 8 (longer segments
+// lengthen the accumulation chains, shorter ones add heads and merge levels).
 static uint32_t auto_seg_len(size_t n, uint32_t windows) {
   const double entries = (double)n * windows;
   if (entries < (double)(1u << 19)) return 8;
-  if (entries < (double)(1u << 21)) return 16;
   if (entries < (double)(1u << 23)) return 32;
   if (entries < (double)(1u << 26)) return 64;
   return 128;
@@ -85,6 +85,7 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
     set_scan_smem_limits();
   }
   glv = glv_default();
+  chunk = std::min(n, max_chunk());
   layout();
   result.alloc(xyzz_words(), "msm result");
   result_handle.ctx = ctx;
@@ -94,15 +95,31 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   check_cuda(cudaMemsetAsync(result.ptr, 0, xyzz_words() * 4, ctx->stream), "msm result init");
 }
 
+size_t MsmPlan::max_chunk() const {
+  // fewer than 2^32 - 1 (window, point) entries per pass; GLV: 2 chunk points below 2^31 too
+  if (glv) return std::min<size_t>(0xfffffffeull / (2 * ((128 + c - 1) / c)), ((size_t)kNegBit >> 1) - 1);
+  return 0xfffffffeull / ((255 + c - 1) / c);
+}
+
+void MsmPlan::set_chunk(size_t points) {
+  if (fixed_base) fail(ZKG_EINVAL, "a fixed-base plan runs in one pass");
+  use(ctx);
+  chunk_req = points;
+  const size_t want = std::min(n, std::min(points ? points : n, max_chunk()));
+  if (want != chunk) {
+    chunk = want;
+    layout();
+  }
+}
+
 void MsmPlan::layout() {
-  const size_t np = points();
+  const size_t np = glv ? 2 * chunk : chunk;  // points of the largest pass
   windows = glv ? (128 + c - 1) / c : (255 + c - 1) / c;
   half = 1u << (c - 1);
   slots = (size_t)windows * half;
   seg_len = item_points_req ? item_points_req : auto_seg_len(np, windows);
   const size_t xw = xyzz_words();
   const size_t max_entries = (size_t)windows * np;
-  if (max_entries >= 0xffffffffull) fail(ZKG_EINVAL, "windows * n must stay below 2^32 entries");
 
   counts.alloc(slots, "msm counts");
   slot_start.alloc(slots + 1, "msm slot_start");
@@ -168,8 +185,10 @@ void MsmPlan::layout() {
   runs[0].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   runs[1].alloc(std::max<size_t>(run_points, 1) * xw, "msm runs");
   window_sums.alloc((size_t)windows * xw, "msm window sums");
-  if (glv) glv_bases.alloc(n * affine_words(), "msm GLV bases (phi)");
+  if (glv) glv_bases.alloc(chunk * affine_words(), "msm GLV bases (phi)");
   else glv_bases.release();
+  if (passes() > 1) partial.alloc(xw, "msm pass result");
+  else partial.release();
 }
 
 size_t MsmPlan::xyzz_words() const { return group == ZKG_G1 ? 32 : 64; }
@@ -193,8 +212,7 @@ void MsmPlan::check_buffers(const zkg_buf* bases, const zkg_buf* scalars) const 
 // 2^22: 15.7 / 16.7; 2^24: 54.8 / 55.1), half the reduction and combination work for the same
 // bucket additions.
 bool MsmPlan::glv_default() const {
-  return group == ZKG_G1 && c <= 16 && 2 * n < (size_t)kNegBit &&
-         (double)((128 + c - 1) / c) * 2.0 * (double)n < 4294967295.0;
+  return group == ZKG_G1 && c <= 16;
 }
 
 void MsmPlan::set_glv(bool enable) {
@@ -203,15 +221,17 @@ void MsmPlan::set_glv(bool enable) {
     if (group != ZKG_G1) fail(ZKG_EINVAL, "GLV splitting is for G1 (the endomorphism (x, y) -> (beta x, y))");
     if (c > 16) fail(ZKG_EINVAL, "GLV splitting needs a window size c <= 16, got " + std::to_string(c));
     if (fixed_base) fail(ZKG_EINVAL, "GLV splitting and fixed-base tables do not combine");
-    if (2 * n >= (size_t)kNegBit) fail(ZKG_EINVAL, "a GLV MSM holds fewer than 2^30 points");
   }
   use(ctx);
   const bool old = glv;
+  const size_t old_chunk = chunk;
   glv = enable;
   try {
+    chunk = std::min(n, std::min(chunk_req ? chunk_req : n, max_chunk()));
     layout();
   } catch (...) {
     glv = old;
+    chunk = old_chunk;
     layout();
     throw;
   }
@@ -223,6 +243,10 @@ void MsmPlan::set_fixed_base(bool enable) {
   if (enable && plain_windows * n >= (size_t)kNegBit)
     fail(ZKG_EINVAL, "a fixed-base table holds fewer than 2^31 points");
   if (enable && glv) set_glv(false);  // the table's rows are the plain windows
+  if (enable && chunk != n) {  // one pass: the table's rows are n points apart
+    chunk = n;
+    layout();
+  }
   fixed_base = enable;
 }
 
@@ -247,13 +271,13 @@ template <int AGG>
 void MsmPlan::rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
   const unsigned b256 = 256;
   if (glv) {
-    msm_glv_phi<<<grid_for(n, b256), b256, 0, s>>>(bases, n, glv_bases.ptr);
+    msm_glv_phi<<<grid_for(run_n, b256), b256, 0, s>>>(bases, run_n, glv_bases.ptr);
     check_launch("msm_glv_phi");
-    msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), n, c, windows, 0, counts.ptr,
-                                                                   digits.as<uint16_t>(), ranks.ptr);
+    msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), run_n, c, windows, 0,
+                                                                   counts.ptr, digits.as<uint16_t>(), ranks.ptr);
   } else {
-    msm_rank<AGG, false><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, n, c, windows, fixed_base, counts.ptr,
-                                                             digits.as<uint16_t>(), ranks.ptr);
+    msm_rank<AGG, false><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, run_n, c, windows, fixed_base,
+                                                                 counts.ptr, digits.as<uint16_t>(), ranks.ptr);
   }
 }
 
@@ -274,13 +298,13 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
           rank<3>(bases, scalars, s);
         check_launch("msm_rank");
       } else if (sort_agg == 1)
-        msm_count<1><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+        msm_count<1><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, counts.ptr);
       else if (sort_agg == 2)
-        msm_count<2><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+        msm_count<2><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, counts.ptr);
       else if (sort_agg == 3)
-        msm_count<3><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+        msm_count<3><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, counts.ptr);
       else
-        msm_count<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, counts.ptr);
+        msm_count<0><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, counts.ptr);
       check_launch("msm_count");
       break;
     case kStageScan:
@@ -305,13 +329,13 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
         break;
       }
       // every group merged: measured best or equal for the scatter on every distribution
-      msm_scatter<0><<<grid_for(n, b256), b256, 0, s>>>(scalars, n, c, windows, cursor.ptr, sorted.ptr);
+      msm_scatter<0><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, cursor.ptr, sorted.ptr);
       check_launch("msm_scatter");
       break;
     case kStageAccumulate: {
-      // GLV: points n..2n-1 are the phi(P_i) of glv_bases
+      // GLV: points run_n..2 run_n - 1 are the phi(P_i) of glv_bases
       const uint32_t* bases2 = glv ? glv_bases.ptr : bases;
-      const uint32_t split = glv ? (uint32_t)n : 0xffffffffu;
+      const uint32_t split = glv ? (uint32_t)run_n : 0xffffffffu;
       if ((acc_variant == 5 || acc_variant == 6) && std::is_same<F, Fq>::value) {
         // G1 with the accumulator in shared memory, four blocks per SM
         const size_t acc_smem = f64_acc_smem<f64::FqD>(true);
@@ -350,12 +374,16 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
       // lane: 2^16 with GLV 0.287 -> 0.265 ms); G2 keeps the out-of-line Fq2 products.
       if constexpr (std::is_same<F, Fq>::value)
         msm_combine_lanes<Fq><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(), glv ? 128u / windows : c,
-                                               glv ? 128u % windows : 0u, result.ptr);
+                                               glv ? 128u % windows : 0u, combine_out);
       else
         msm_combine_lanes<typename CompactOf<F>::type><<<1, 32, 0, s>>>(window_sums.ptr, active_windows(),
                                                                          glv ? 128u / windows : c,
-                                                                         glv ? 128u % windows : 0u, result.ptr);
+                                                                         glv ? 128u % windows : 0u, combine_out);
       check_launch("msm_combine_lanes");
+      if (!first_pass) {  // a later pass: add its point into the result
+        msm_add_partial<F><<<1, 32, 0, s>>>(result.ptr, partial.ptr);
+        check_launch("msm_add_partial");
+      }
       break;
     case kStageMerge:
     case kStageReduce:
@@ -426,12 +454,26 @@ const char* MsmPlan::stage_name(int which) {
   return names[which];
 }
 
+// Selects pass `off` (its first point): run_n, where the combination writes, and the pass's
+// slice of the bases (a fixed-base plan has one pass) and scalars.
+void MsmPlan::begin_pass(size_t off, const uint32_t*& bases, const uint32_t*& scalars) {
+  run_n = std::min(chunk, n - off);
+  first_pass = off == 0;
+  combine_out = first_pass ? result.ptr : partial.ptr;
+  bases += off * affine_words();
+  scalars += off * 8;
+}
+
 void MsmPlan::enqueue(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s) {
-  for (int st = 0; st < kStages; st++) {
-    size_t ev = timer.enabled ? timer.begin(st, s) : 0;
-    if (group == ZKG_G1) stage<Fq>(st, bases, scalars, s);
-    else stage<Fq2>(st, bases, scalars, s);
-    if (timer.enabled) timer.end(ev, s);
+  for (size_t off = 0; off < n; off += chunk) {
+    const uint32_t *b = bases, *sc = scalars;
+    begin_pass(off, b, sc);
+    for (int st = 0; st < kStages; st++) {
+      size_t ev = timer.enabled ? timer.begin(st, s) : 0;
+      if (group == ZKG_G1) stage<Fq>(st, b, sc, s);
+      else stage<Fq2>(st, b, sc, s);
+      if (timer.enabled) timer.end(ev, s);
+    }
   }
   if (timer.enabled) timer.runs++;
 }
@@ -449,15 +491,20 @@ std::vector<std::pair<std::string, double>> MsmPlan::profile(const zkg_buf* base
   cudaEvent_t a, b;
   check_cuda(cudaEventCreate(&a), "event");
   check_cuda(cudaEventCreate(&b), "event");
-  for (int st = 0; st < kStages; st++) {
-    check_cuda(cudaEventRecord(a, ctx->stream), "event record");
-    if (group == ZKG_G1) stage<Fq>(st, bases->ptr, scalars->ptr, ctx->stream);
-    else stage<Fq2>(st, bases->ptr, scalars->ptr, ctx->stream);
-    check_cuda(cudaEventRecord(b, ctx->stream), "event record");
-    check_cuda(cudaEventSynchronize(b), "msm stage");
-    float ms = 0;
-    check_cuda(cudaEventElapsedTime(&ms, a, b), "event time");
-    out.emplace_back(stage_name(st), (double)ms);
+  for (int st = 0; st < kStages; st++) out.emplace_back(stage_name(st), 0.0);
+  for (size_t off = 0; off < n; off += chunk) {  // stage times summed over the passes
+    const uint32_t *bp = bases->ptr, *sp = scalars->ptr;
+    begin_pass(off, bp, sp);
+    for (int st = 0; st < kStages; st++) {
+      check_cuda(cudaEventRecord(a, ctx->stream), "event record");
+      if (group == ZKG_G1) stage<Fq>(st, bp, sp, ctx->stream);
+      else stage<Fq2>(st, bp, sp, ctx->stream);
+      check_cuda(cudaEventRecord(b, ctx->stream), "event record");
+      check_cuda(cudaEventSynchronize(b), "msm stage");
+      float ms = 0;
+      check_cuda(cudaEventElapsedTime(&ms, a, b), "event time");
+      out[st].second += (double)ms;
+    }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);

@@ -68,7 +68,16 @@ struct MsmPlan {
   // switches it off.
   bool glv = false;
   bool glv_default() const;
-  size_t points() const { return glv ? 2 * n : n; }
+  // Points per pass. Entry positions and point indices are 32-bit, so one pass holds fewer than
+  // 2^32 (window, point) entries; a run over more points goes in passes of `chunk` points whose
+  // results are added (the reference's limit, n < 2^31, is kept). The plan's scratch is sized
+  // for one pass, so a smaller chunk (zkg_msm_set_chunk) also bounds its device memory.
+  size_t chunk = 0, run_n = 0;  // run_n: the points of the pass being queued
+  size_t chunk_req = 0;         // 0: the largest pass the mode allows
+  size_t max_chunk() const;
+  void set_chunk(size_t points);
+  size_t passes() const { return (n + chunk - 1) / chunk; }
+  size_t points() const { return glv ? 2 * run_n : run_n; }
   size_t active_slots() const { return fixed_base ? half : slots; }
   uint32_t active_windows() const { return fixed_base ? 1u : windows; }
   size_t slots = 0, heads_max = 0;
@@ -80,7 +89,7 @@ struct MsmPlan {
   DeviceArray ranks, digits;  // the ranked sort's rank (32 bits) and digit (16 bits) per (window, point), window-major
   DeviceArray glv_bases;      // GLV mode: phi(P_0)..phi(P_{n-1})
   DeviceArray heads[2], head_keys[2];
-  DeviceArray tots, runs[2], window_sums, result;
+  DeviceArray tots, runs[2], window_sums, result, partial;  // partial: a later pass's result
   zkg_buf result_handle;
   StageTimer timer;
 
@@ -110,6 +119,9 @@ struct MsmPlan {
   // Windows, slots, segments, merge and reduction levels and their scratch, for the current
   // mode (points() and the scalar width); the result buffer is kept.
   void layout();
+  uint32_t* combine_out = nullptr;  // where the combination of the pass being queued goes
+  bool first_pass = true;
+  void begin_pass(size_t off, const uint32_t*& bases, const uint32_t*& scalars);
   template <int AGG>
   void rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t s);
   uint32_t item_points_req = 0;

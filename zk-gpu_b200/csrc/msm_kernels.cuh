@@ -863,6 +863,14 @@ __global__ void __launch_bounds__(32) msm_combine_lanes(const uint32_t* __restri
   if (threadIdx.x == 0) store_xyzz(result, acc);
 }
 
+// result <- result + partial (XYZZ, one thread): the passes of a run over more points than one
+// pass holds.
+template <class F>
+__global__ void msm_add_partial(uint32_t* __restrict__ result, const uint32_t* __restrict__ partial) {
+  if (threadIdx.x != 0) return;
+  store_xyzz(result, xyzz_add(load_xyzz<F>(result), load_xyzz<F>(partial)));
+}
+
 // ------------------------------------------------------------------ base upload
 
 // x <- x * scale / 2^256 for every 8-word Fq coordinate (to_montgomery.wgsl:6-15). With

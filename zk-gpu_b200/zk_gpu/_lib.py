@@ -74,6 +74,8 @@ SIGNATURES = {
                                                 ctypes.POINTER(vp)]),
     "zkg_msm_set_fixed_base": (ctypes.c_int, [vp, ctypes.c_int]),
     "zkg_msm_set_glv": (ctypes.c_int, [vp, ctypes.c_int]),
+    "zkg_msm_set_chunk": (ctypes.c_int, [vp, ctypes.c_size_t]),
+    "zkg_msm_passes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     "zkg_msm_windows": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int)]),
     "zkg_xyzz_add_host": (ctypes.c_int, [ctypes.c_int, u32p, u32p, u32p]),
     "zkg_quotient": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_uint32, u32p]),

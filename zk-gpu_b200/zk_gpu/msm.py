@@ -83,6 +83,17 @@ class Msm:
         check(lib().zkg_msm_fixed_base_table(gpu.handle, int(group), bases.handle, n, c, ctypes.byref(h)))
         return Buffer(gpu, h.value)
 
+    def set_chunk(self, points: int) -> None:
+        """Run in passes of at most `points` points (0: the largest the 32-bit entry indices
+        allow); bounds the plan's scratch memory. The result does not change."""
+        check(lib().zkg_msm_set_chunk(self._h, points))
+
+    def passes(self) -> tuple[int, int]:
+        """(points per pass, passes per run)."""
+        ch, ps = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib().zkg_msm_passes(self._h, ctypes.byref(ch), ctypes.byref(ps)))
+        return ch.value, ps.value
+
     def set_glv(self, enable: bool = True) -> None:
         """G1: split every scalar as k1 + k2 lambda (mod r) and run over P_i and phi(P_i) with
         ceil(128 / c) windows; the same result as the plain MSM."""
