@@ -156,7 +156,7 @@ void MsmPlan::layout() {
   // Running-sum levels: m_0 = B; m_{l+1} = ceil(m_l / C) - 1 while positive (C = 2^chunk_log).
   std::memset(&levels, 0, sizeof(levels));
   levels.chunk_log = chunk_log;
-  const uint32_t chunk = 1u << chunk_log;
+  const uint32_t bucket_chunk = 1u << chunk_log;
   uint32_t m = half;
   size_t tot_points = 0, run_points = 0;
   std::vector<uint32_t> ms;
@@ -170,7 +170,7 @@ void MsmPlan::layout() {
       levels.count++;
       break;
     }
-    uint32_t chunks = (m + chunk - 1) / chunk;
+    uint32_t chunks = (m + bucket_chunk - 1) / bucket_chunk;
     uint32_t blocks = (chunks + kReduceThreads - 1) / kReduceThreads;  // one tot point per block
     ms.push_back(m);
     levels.tot_len[levels.count] = blocks;
