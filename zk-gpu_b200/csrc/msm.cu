@@ -273,11 +273,11 @@ void MsmPlan::rank(const uint32_t* bases, const uint32_t* scalars, cudaStream_t 
   if (glv) {
     msm_glv_phi<<<grid_for(run_n, b256), b256, 0, s>>>(bases, run_n, glv_bases.ptr);
     check_launch("msm_glv_phi");
-    msm_rank<AGG, true><<<grid_for(points(), b256), b256, 0, s>>>(scalars, points(), run_n, c, windows, 0,
-                                                                   counts.ptr, digits.as<uint16_t>(), ranks.ptr);
+    msm_rank_glv<AGG><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, counts.ptr,
+                                                              digits.as<uint16_t>(), ranks.ptr);
   } else {
-    msm_rank<AGG, false><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, run_n, c, windows, fixed_base,
-                                                                 counts.ptr, digits.as<uint16_t>(), ranks.ptr);
+    msm_rank<AGG><<<grid_for(run_n, b256), b256, 0, s>>>(scalars, run_n, c, windows, fixed_base, counts.ptr,
+                                                          digits.as<uint16_t>(), ranks.ptr);
   }
 }
 

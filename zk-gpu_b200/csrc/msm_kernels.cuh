@@ -77,15 +77,31 @@ struct Recoder {
     }
     return mag ? w * half + mag - 1 : kNoKey;
   }
-  // The same for a window of `width` bits starting at bit `pos` (width <= c: the GLV windows),
-  // the digit negated when `flip` (a negative half-scalar: its digits are those of |k| with the
+};
+
+// Recoding of a GLV half (127-bit magnitude in four words; the words are picked by selects, so
+// two of these stay in registers in one thread).
+struct GlvRecoder {
+  uint32_t s[4];
+  uint32_t carry = 0;
+  __device__ __forceinline__ uint32_t word(uint32_t i) const {
+    return i == 0 ? s[0] : i == 1 ? s[1] : i == 2 ? s[2] : i == 3 ? s[3] : 0u;
+  }
+  __device__ __forceinline__ uint32_t window_bits(uint32_t pos, uint32_t width) const {
+    const uint32_t wd = pos >> 5, off = pos & 31;
+    uint32_t v = word(wd) >> off;
+    if (off + width > 32) v |= word(wd + 1) << (32 - off);
+    return v & ((1u << width) - 1);
+  }
+  // Recoder::next for a window of `width` bits starting at bit `pos` (width <= c: the GLV
+  // windows), the digit negated when `flip` (a negative half-scalar: its digits are those of |k| with the
   // sign turned). A flipped half is recoded with v > 2^(width-1) negative instead of >=, so its
   // digits lie in (-2^(width-1), 2^(width-1)] and, turned, in [-2^(width-1), 2^(width-1)) like
   // every other digit: the positive magnitude 2^(c-1), whose 16-bit code is kRankZero at c = 16,
   // never occurs.
   __device__ __forceinline__ uint32_t next_at(uint32_t w, uint32_t pos, uint32_t width, uint32_t half, bool flip,
                                               bool* neg) {
-    const uint32_t v = window_bits(s, pos, width) + carry;
+    const uint32_t v = window_bits(pos, width) + carry;
     const uint32_t h = 1u << (width - 1);
     carry = 0;
     uint32_t mag = v;
@@ -284,10 +300,27 @@ __device__ __forceinline__ void round_quotient(const uint64_t (&k)[4], const uin
   for (int i = 0; i < LC; i++) c[i] = p[4 + i];
 }
 
+// |v| (a signed 192-bit value, |v| < 2^127) into out (words 0..3; 4..7 zero); whether v < 0.
+__device__ __forceinline__ bool store_half(uint64_t (&v)[3], uint32_t out[8]) {
+  const bool neg = v[2] >> 63;
+  if (neg) {
+    uint64_t m[3] = {0, 0, 0};
+    sub_mod(m, v);
+    v[0] = m[0];
+    v[1] = m[1];
+  }
+  out[0] = (uint32_t)v[0];
+  out[1] = (uint32_t)(v[0] >> 32);
+  out[2] = (uint32_t)v[1];
+  out[3] = (uint32_t)(v[1] >> 32);
+#pragma unroll
+  for (int i = 4; i < 8; i++) out[i] = 0;
+  return neg;
+}
+
 // s (8 words, any 256-bit value; reduced mod r first, which changes no multiple of a point of
-// G1) -> |k1| (second = false) or |k2| (second = true) in words 0..3, words 4..7 zero; returns
-// whether that half is negative.
-__device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
+// G1) -> |k1| in k1, |k2| in k2 (words 0..3, words 4..7 zero) and their signs.
+__device__ __forceinline__ void split(const uint32_t s[8], uint32_t k1[8], bool& neg1, uint32_t k2[8], bool& neg2) {
   uint64_t k[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) k[i] = s[2 * i] | (uint64_t)s[2 * i + 1] << 32;
@@ -310,35 +343,26 @@ __device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
   uint64_t c1[2], c2[1];
   round_quotient(k, kG1, c1);  // < b2 + 1 < 2^127
   round_quotient(k, kG2, c2);  // < -b1 + 1 < 2^64
-  uint64_t v[3], t[3];
-  if (!second) {  // k1 = k - c1 a1 - c2 a2
-    v[0] = k[0];
-    v[1] = k[1];
-    v[2] = k[2];
-    mul_lo<3>(c1, kA1, t);
-    sub_mod(v, t);
-    mul_lo<3>(c2, kShort, t);
-    sub_mod(v, t);
-  } else {  // k2 = c1 (-b1) - c2 b2
-    mul_lo<3>(c1, kShort, v);
-    mul_lo<3>(c2, kB2, t);
-    sub_mod(v, t);
-  }
-  const bool neg = v[2] >> 63;
-  if (neg) {
-    const uint64_t zero[3] = {0, 0, 0};
-    uint64_t m[3] = {zero[0], zero[1], zero[2]};
-    sub_mod(m, v);
-    v[0] = m[0];
-    v[1] = m[1];
-  }
-  s[0] = (uint32_t)v[0];
-  s[1] = (uint32_t)(v[0] >> 32);
-  s[2] = (uint32_t)v[1];
-  s[3] = (uint32_t)(v[1] >> 32);
+  uint64_t v[3] = {k[0], k[1], k[2]}, t[3];  // k1 = k - c1 a1 - c2 a2
+  mul_lo<3>(c1, kA1, t);
+  sub_mod(v, t);
+  mul_lo<3>(c2, kShort, t);
+  sub_mod(v, t);
+  neg1 = store_half(v, k1);
+  mul_lo<3>(c1, kShort, v);  // k2 = c1 (-b1) - c2 b2
+  mul_lo<3>(c2, kB2, t);
+  sub_mod(v, t);
+  neg2 = store_half(v, k2);
+}
+
+// One half of split: s -> |k1| (second = false) or |k2| (second = true), returning its sign.
+__device__ __forceinline__ bool split_half(uint32_t s[8], bool second) {
+  uint32_t h1[8], h2[8];
+  bool n1, n2;
+  split(s, h1, n1, h2, n2);
 #pragma unroll
-  for (int i = 4; i < 8; i++) s[i] = 0;
-  return neg;
+  for (int i = 0; i < 8; i++) s[i] = second ? h2[i] : h1[i];
+  return second ? n2 : n1;
 }
 }  // namespace glv
 
@@ -374,26 +398,14 @@ constexpr uint32_t kRankZero = 0x7fffu;  // a positive bucket 2^15 - 1 never occ
 
 // fixed (fixed-base tables: one set of buckets for all windows, see msm_place): the digit of
 // window w counts in bucket slot |d| - 1 instead of w * 2^(c-1) + |d| - 1.
-// GLV: n = 2 scalar_n points; entry i < scalar_n takes |k1| of scalar i (base P_i), entry
-// scalar_n + i takes |k2| of scalar i (base phi(P_i)), each with its half's sign folded into its
-// digits (glv::split_half, Recoder::next_at).
-template <int AGG, bool GLV = false>
-__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t scalar_n, uint32_t c, uint32_t windows,
-                         int fixed, uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
+template <int AGG>
+__global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, uint32_t c, uint32_t windows, int fixed,
+                         uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
                          uint32_t* __restrict__ ranks) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < n;
   Recoder rc;
-  bool flip = false;
-  if (live) {
-    if (GLV) {
-      const bool second = i >= scalar_n;
-      load_scalar(scalars, second ? i - scalar_n : i, rc.s);
-      flip = glv::split_half(rc.s, second);
-    } else {
-      load_scalar(scalars, i, rc.s);
-    }
-  }
+  if (live) load_scalar(scalars, i, rc.s);
   const uint32_t half = 1u << (c - 1);
   const unsigned lane = threadIdx.x & 31;
   // Windows four at a time: the four counting atomics (each returns the entry's rank) are in
@@ -409,9 +421,7 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t 
       slot[k] = kNoKey;
       neg[k] = false;
       if (w < windows) {  // uniform across the warp
-        if (live)
-          slot[k] = GLV ? rc.next_at(w, glv_window_pos(w, windows), glv_window_width(w, windows), half, flip, &neg[k])
-                        : rc.next(w, c, half, &neg[k]);
+        if (live) slot[k] = rc.next(w, c, half, &neg[k]);
         if (fixed && slot[k] != kNoKey) slot[k] -= w * half;
         peers[k] = slot_peers<AGG>(slot[k]);
         base[k] = 0;
@@ -432,6 +442,78 @@ __global__ void msm_rank(const uint32_t* __restrict__ scalars, size_t n, size_t 
         __stcs(ranks + e, b + __popc(peers[k] & ((1u << lane) - 1)));  // streamed: read once by msm_place
       }
       __stcs(digits + e, (unsigned short)code);
+    }
+  }
+}
+
+// The GLV counting pass, one thread per scalar: thread i splits scalar i once (glv::split) and
+// recodes both halves, entry i (|k1|, base P_i) and entry scalar_n + i (|k2|, base phi(P_i)),
+// each half's sign folded into its digits; entries are window-major over 2 scalar_n points, as
+// msm_place reads them. Two windows per batch: four counting atomics in flight.
+template <int AGG>
+__global__ void msm_rank_glv(const uint32_t* __restrict__ scalars, size_t scalar_n, uint32_t c, uint32_t windows,
+                             uint32_t* __restrict__ counts, uint16_t* __restrict__ digits,
+                             uint32_t* __restrict__ ranks) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < scalar_n;
+  const size_t n = 2 * scalar_n;
+  GlvRecoder rc[2];
+  bool flip[2] = {false, false};
+  if (live) {
+    uint32_t s[8], h1[8], h2[8];
+    load_scalar(scalars, i, s);
+    glv::split(s, h1, flip[0], h2, flip[1]);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      rc[0].s[j] = h1[j];
+      rc[1].s[j] = h2[j];
+    }
+  }
+  const uint32_t half = 1u << (c - 1);
+  const unsigned lane = threadIdx.x & 31;
+  constexpr int kBatch = 2;
+  for (uint32_t w0 = 0; w0 < windows; w0 += kBatch) {
+    uint32_t slot[kBatch][2], base[kBatch][2];
+    unsigned peers[kBatch][2];
+    bool neg[kBatch][2];
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const uint32_t w = w0 + k;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        slot[k][h] = kNoKey;
+        neg[k][h] = false;
+        peers[k][h] = 0;
+        base[k][h] = 0;
+        if (w < windows) {  // uniform across the warp
+          if (live)
+            slot[k][h] = rc[h].next_at(w, glv_window_pos(w, windows), glv_window_width(w, windows), half, flip[h],
+                                       &neg[k][h]);
+          peers[k][h] = slot_peers<AGG>(slot[k][h]);
+          if (peers[k][h] && (int)lane == __ffs(peers[k][h]) - 1)
+            base[k][h] = atomicAdd(&counts[slot[k][h]], (uint32_t)__popc(peers[k][h]));
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const uint32_t w = w0 + k;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (w < windows) {
+          const int leader = peers[k][h] ? __ffs(peers[k][h]) - 1 : (int)lane;
+          const uint32_t b = __shfl_sync(0xffffffffu, base[k][h], leader);
+          if (live) {
+            uint32_t code = kRankZero;
+            const size_t e = (size_t)w * n + i + (h ? scalar_n : 0);
+            if (peers[k][h]) {
+              code = (slot[k][h] - w * half) | (neg[k][h] ? 0x8000u : 0u);
+              __stcs(ranks + e, b + __popc(peers[k][h] & ((1u << lane) - 1)));
+            }
+            __stcs(digits + e, (unsigned short)code);
+          }
+        }
+      }
     }
   }
 }
