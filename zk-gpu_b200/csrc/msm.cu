@@ -323,8 +323,8 @@ void MsmPlan::stage(int which, const uint32_t* bases, const uint32_t* scalars, c
     case kStageScatter:
       if (ranked_sort()) {
         const dim3 grid((unsigned)grid_for(points(), b256), windows);
-        msm_place<<<grid, b256, 0, s>>>(digits.as<uint16_t>(), ranks.ptr, points(), half, fixed_base, slot_start.ptr,
-                                        sorted.ptr);
+        msm_place<<<grid, b256, 0, s>>>(digits.as<uint16_t>(), ranks.ptr, points(), half, fixed_base, glv ? 1 : 0,
+                                        slot_start.ptr, sorted.ptr);
         check_launch("msm_place");
         break;
       }
