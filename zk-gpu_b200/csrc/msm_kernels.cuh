@@ -501,20 +501,19 @@ __global__ void msm_rank_glv(const uint32_t* __restrict__ scalars, size_t scalar
 #pragma unroll
     for (int k = 0; k < kBatch; k++) {
       const uint32_t w = w0 + k;
+      if (w < windows) {
+        uint32_t code[2], rank[2];
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        if (w < windows) {
+        for (int h = 0; h < 2; h++) {
           const int leader = peers[k][h] ? __ffs(peers[k][h]) - 1 : (int)lane;
           const uint32_t b = __shfl_sync(0xffffffffu, base[k][h], leader);
-          if (live) {
-            uint32_t code = kRankZero;
-            const size_t e = (size_t)w * n + 2 * i + h;  // the halves side by side (msm_place)
-            if (peers[k][h]) {
-              code = (slot[k][h] - w * half) | (neg[k][h] ? 0x8000u : 0u);
-              __stcs(ranks + e, b + __popc(peers[k][h] & ((1u << lane) - 1)));
-            }
-            __stcs(digits + e, (unsigned short)code);
-          }
+          code[h] = peers[k][h] ? (slot[k][h] - w * half) | (neg[k][h] ? 0x8000u : 0u) : kRankZero;
+          rank[h] = b + __popc(peers[k][h] & ((1u << lane) - 1));  // read only for a nonzero digit
+        }
+        if (live) {  // the halves side by side (msm_place), one store each for the pair
+          const size_t e = (size_t)w * n + 2 * i;  // even (n = 2 scalar_n): 4- and 8-byte aligned stores
+          __stcs(reinterpret_cast<uint32_t*>(digits + e), code[0] | code[1] << 16);
+          __stcs(reinterpret_cast<uint2*>(ranks + e), make_uint2(rank[0], rank[1]));
         }
       }
     }
