@@ -40,10 +40,10 @@ IMAD_PER_MULMOD = 264  # 8 rows x (16 product + 16 reduction multiply-adds + 1 m
 FP64_PER_MULMOD = 170  # double-precision instructions per Fq product in limb form, field_f64.cuh
 MULMODS_PER_MADD = 10  # madd-2008-s: 8M + 2S
 # ncu DRAM traffic (read + write bytes) per launch. msm_accumulate_f64: captured on a G1 MSM of
-# 2^22 points (7.05 GB) and scaled by the entry count to 2^24 (x4); NTT forms 0, 1 and 2: the
-# first pass captured on the 2^24 transform.
+# 2^22 points with the default plan (GLV split: 8.14 GB read + 0.11 GB written) and scaled by the
+# entry count to 2^24 (x4); NTT forms 0, 1 and 2: the first pass captured on the 2^24 transform.
 NCU_TRAFFIC = {
-    "msm_accumulate_2^24": 28.2e9,
+    "msm_accumulate_2^24": 33.0e9,
     "ntt_form0_2^24": 1.96e9,
     "ntt_form1_2^24": 2.18e9,
     "ntt_form2_2^24": 1.71e9,
