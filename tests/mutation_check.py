@@ -33,6 +33,7 @@ MUTANTS = [
      "for (uint32_t k = 1; k < width; k++) acc = lane_double(acc, sm);"),
     ("glv-round", CSRC + "msm_kernels.cuh", "const uint64_t t = p[3] + (1ull << 63);", "const uint64_t t = p[3];"),
     ("glv-sign", CSRC + "msm_kernels.cuh", "    *neg = neg_d != flip;", "    *neg = neg_d;"),
+    ("glv-digits-carry", CSRC + "msm_kernels.cuh", "      neg_d = true;\n      carry = 1;", "      neg_d = true;"),
     ("sort-sign", CSRC + "msm_kernels.cuh", "code = (fixed ? slot[k] : slot[k] - w * half) | (neg[k] ? 0x8000u : 0u);",
      "code = (fixed ? slot[k] : slot[k] - w * half) | 0u;"),
     ("reduce-weights", CSRC + "msm_kernels.cuh",
