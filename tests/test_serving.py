@@ -145,6 +145,27 @@ def test_reserved_slots_serve_a_burst_without_new_slots(gpu, key):
     server.close()
 
 
+def test_busy_slots_of_a_size_are_waited_for(gpu, key):
+    """A size that has its reserved slots (at least two) all busy does not get another built:
+    its next requests wait for them (a build under load costs more than the wait); an unreserved
+    size gets at most two. All requests complete with the plain path's results."""
+    sizes = [11] * 6 + [12] * 5
+    reqs = [make_request(lm, 9000 + 19 * i) for i, lm in enumerate(sizes)]
+    alone = run_plain(gpu, key, [make_request(lm, 9000 + 19 * i) for i, lm in enumerate(sizes)])
+    server = Server(gpu, lanes=6, coset_g=G)
+    server.add_key(KEY_N, key[2], key[3])
+    server.reserve(11, 2)
+    ids = [server.submit(r) for r in reqs]  # all at once: more same-size requests than slots
+    for rid in ids:
+        server.wait(rid)
+    stats = server.stats()
+    assert stats["completed"] == len(reqs)
+    assert stats["slots_created"] == 4, stats  # two reserved for 2^11, two built for 2^12
+    for i, r in enumerate(reqs):
+        assert same_points(affine_points(r.points()), alone[i][0]) and np.array_equal(r.h(), alone[i][1]), i
+    server.close()
+
+
 def test_requests_with_slots_pass_one_whose_slot_is_being_made(gpu, key):
     """A request that needs a new slot does not hold back later requests whose slots exist: all
     complete, with the plain path's results."""

@@ -272,9 +272,12 @@ void Server::launch(ServerRequest* r, ServerSlot* s) {
 }
 
 // Admission. The queue is scanned in order while lanes are free: a request with an idle slot of
-// its size is launched at once; one without gets a slot built for it by the builder thread when
-// the slot fits the HBM budget (after evicting idle slots of other sizes, oldest first), and
-// the scan goes on, so requests whose slots exist are not held up by a slot under construction.
+// its size is launched at once; one without waits for a busy slot of its size when the size
+// already has max(2, reserved) slots (built or being built), and otherwise gets a slot built for
+// it by the builder thread when the slot fits the HBM budget (after evicting idle slots of other
+// sizes, oldest first); either way the scan goes on, so requests whose slots exist are not held
+// up by a slot under construction (measured: a slot built under load took 764 ms, a request of
+// the largest size about 120 ms of kernels).
 // A request whose slot does not fit stops the scan (later requests wait behind it in FIFO order)
 // unless nothing is running, in which case its slot is made anyway.
 void Server::dispatcher() {
@@ -299,6 +302,13 @@ void Server::dispatcher() {
               break;
             }
           if (!slot) {
+            uint32_t have = building_of[log_m];
+            for (auto& s : slots) have += s->log_m == log_m ? 1 : 0;
+            const auto rv = reserved.find(log_m);
+            if (have >= std::max<uint32_t>(2, rv == reserved.end() ? 0 : rv->second)) {
+              ++it;  // wait for a slot of this size; later requests of other sizes go on
+              continue;
+            }
             const size_t need = estimate_bytes(log_m);
             for (size_t i = 0; i < slots.size() && bytes_used + need > budget;) {
               if (!slots[i]->busy && slots[i]->log_m != log_m) {
@@ -314,6 +324,7 @@ void Server::dispatcher() {
             bytes_used += need;
             builds.emplace_back(r, need);
             building++;
+            building_of[log_m]++;
             new_builds = true;
           } else {
             slot->busy = true;
@@ -373,6 +384,7 @@ void Server::builder() {
         bytes_used = bytes_used - std::min(bytes_used, job.second) + s->bytes;
         slots_created++;
         building--;
+        building_of[r->desc.log_m]--;
         s->busy = true;
         s->req = r;
         r->slot = s.get();
@@ -386,6 +398,7 @@ void Server::builder() {
       if (!slot) {
         bytes_used -= std::min(bytes_used, job.second);
         building--;
+        building_of[r->desc.log_m]--;
       } else {
         slot->busy = false;
         slot->req = nullptr;
@@ -403,6 +416,10 @@ void Server::builder() {
 void Server::reserve(uint32_t log_m, uint32_t count) {
   if (log_m < 11 || log_m > 26) fail(ZKG_EINVAL, "log_m must be in 11..=26");
   if (!key_for(log_m)) fail(ZKG_EINVAL, "no resident proving key has 2^" + std::to_string(log_m) + " points");
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    reserved[log_m] = std::max(reserved[log_m], count);
+  }
   for (;;) {
     size_t need = 0;
     {

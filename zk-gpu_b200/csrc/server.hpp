@@ -65,6 +65,10 @@ struct Server {
   // admitted requests whose slot is being made, with the bytes reserved for it
   std::deque<std::pair<ServerRequest*, size_t>> builds;
   int building = 0;  // slots under construction (each holds a lane)
+  // Per size: slots reserved by reserve(), slots under construction. A request whose size has
+  // max(2, reserved) slots (built or being built), all busy, waits for one of them instead of
+  // having another built: under load a build takes tens to hundreds of ms, longer than the wait.
+  std::map<uint32_t, uint32_t> reserved, building_of;
   size_t bytes_used = 0, budget = 0;
   uint64_t next_id = 1;
   uint64_t slots_created = 0, slots_evicted = 0, completed = 0;
