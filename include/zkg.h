@@ -411,7 +411,8 @@ void zkg_host_free(void *p);
 int zkg_msm_set_timing(zkg_msm *msm, int enable);
 int zkg_msm_stage_times(zkg_msm *msm, zkg_stage_time *out, size_t cap, size_t *count, size_t *runs);
 /* Number of (point, window) entries with a nonzero digit in the last run (blocking): the
- * mixed additions the accumulation performed, for throughput accounting. */
+ * mixed additions the accumulation performed, for throughput accounting (for a plan that runs
+ * in passes, zkg_msm_passes, those of the last pass). */
 int zkg_msm_last_entries(zkg_msm *msm, uint64_t *entries);
 /* The same for the NTT: one entry per pass ("pass 0", "pass 1", ...), forward and inverse
  * transforms summed together. */
