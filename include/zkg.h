@@ -122,8 +122,8 @@ int zkg_msm_group(const zkg_msm *msm);
  * products inlined, 1 = products through one out-of-line function (smaller code),
  * 2 = out of line, two independent products per call, 3 / 4 = bucket sums in double-precision
  * limbs, products on the FP64 pipe, two per call / one per call (bit-exact for G1 and G2; the
- * G2 limb forms are slower than the integer pairs). Defaults: for G1 3 below 2^26 (window, point) entries
- * (windows * n) and 4 from there, for G2 2.
+ * G2 limb forms are slower than the integer pairs). Defaults: for G1 4 (with the plain windows, 3
+ * below 2^26 (window, point) entries and 4 from there), for G2 2.
  * zkg_msm_params reports the plan's window c, points per accumulation thread and form. */
 int zkg_msm_set_variant(zkg_msm *msm, int variant);
 /* Counting-sort knob (no reference counterpart): how a warp merges the counting pass's atomics

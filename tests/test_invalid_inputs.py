@@ -68,7 +68,7 @@ def test_tuning_knobs_reject_out_of_range_values(gpu):
     g2 = Msm.for_group(gpu, Group.G2, 1 << 10, 10)
     with pytest.raises(ZkGpuError, match="accumulation variant must be 0..6"):
         g2.set_variant(-1)
-    assert g2.params()["variant"] == 2 and g1.params()["variant"] == 3
+    assert g2.params()["variant"] == 2 and g1.params()["variant"] == 4  # G1: the GLV split's default form
     assert Msm(gpu, 1 << 23, 16).params()["variant"] == 4  # 2^27 entries: one product per call
     ntt = Ntt(gpu, 12)
     with pytest.raises(ZkGpuError, match="NTT variant must be 0..4"):

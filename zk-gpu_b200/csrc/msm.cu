@@ -75,9 +75,6 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
   if (n >= (size_t)kNegBit) fail(ZKG_EINVAL, "an MSM holds fewer than 2^31 points");
   item_points_req = item_points;
   const size_t max_entries = (size_t)((255 + c - 1) / c) * n;
-  // G1: FP64 limbs, two products per call below 2^26 (window, point) entries, one above
-  // (measured: 3.5% faster at 2^20-2^21 points, equal at 2^22, 3.5% slower from 2^23)
-  acc_variant = group == ZKG_G1 ? ((double)max_entries < (double)(1u << 26) ? 3 : 4) : 2;
 
   use(ctx);
   if (group == ZKG_G2) {
@@ -85,6 +82,11 @@ MsmPlan::MsmPlan(zkg_ctx* c_, int group_, size_t n_, uint32_t c, uint32_t item_p
     set_scan_smem_limits();
   }
   glv = glv_default();
+  // G1: FP64 limbs. With the GLV split one product per call at every size (measured: 2^16 1.27
+  // against 1.28 ms for two per call, 2^20 5.48 / 5.58, 2^22 15.60 / 16.05); with the plain
+  // windows two per call below 2^26 (window, point) entries, one above (3.5% faster at 2^20-2^21
+  // points, equal at 2^22, 3.5% slower from 2^23).
+  acc_variant = group == ZKG_G1 ? ((glv || (double)max_entries >= (double)(1u << 26)) ? 4 : 3) : 2;
   chunk = std::min(n, max_chunk());
   layout();
   result.alloc(xyzz_words(), "msm result");

@@ -40,8 +40,9 @@ struct MsmPlan {
   // on instruction fetch; measured 17% faster at 2^24), 2 = out of line, independent products
   // two per call, 3 / 4 = bucket arithmetic in double-precision limbs (msm_f64.cuh), two
   // products per call / one. Every form fetches the next base into shared memory with
-  // cp.async. Defaults (measured on B200): G1 3 below 2^26 (window, point) entries and 4 above
-  // (2^24: 48.1 ms against 50.1 for 3 and 59.7 for 2; 2^20: 3.98 against 4.11 for 4), G2 2
+  // cp.async. Defaults (measured on B200): G1 with the GLV split 4 at every size (2^20: 3.84
+  // against 3.95 ms for 3); G1 with the plain windows 3 below 2^26 (window, point) entries and 4
+  // above (2^24: 48.1 ms against 50.1 for 3 and 59.7 for 2; 2^20: 3.98 against 4.11 for 4), G2 2
   // (47.4 ms at 2^22 against 48.1 for 1 and 55.9 / 63.0 for the limb forms 4 / 3). Tunable.
   int acc_variant = 4;
   // Warp aggregation of the counting pass's atomics (slot_peers in msm_kernels.cuh): 0 = every

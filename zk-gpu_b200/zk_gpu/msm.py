@@ -63,7 +63,8 @@ class Msm:
     def set_variant(self, variant: int) -> None:
         """Accumulation kernel form: 0 inlined field products, 1 out-of-line (smaller code),
         2 out-of-line two at a time; 3 / 4 double-precision limbs, two / one product per call.
-        Defaults: G1 3 below 2^26 (window, point) entries and 4 from there, G2 2."""
+        Defaults: G1 4 (plain windows: 3 below 2^26 (window, point) entries and 4 from there),
+        G2 2."""
         check(lib().zkg_msm_set_variant(self._h, variant))
 
     def set_sort(self, mode: int) -> None:
