@@ -402,15 +402,24 @@ template <class FC>
 void MsmPlan::tail_stage(int which, cudaStream_t s) {
   switch (which) {
     case kStageMerge: {
-      size_t len = heads_max;
-      for (uint32_t l = 0; l < merge_levels; l++) {
+      size_t len = heads_max;  // the largest a level can be (the entry count is on the device)
+      uint32_t l = 0;
+      for (; l < merge_levels; l++) {
         size_t out_len = (len + merge_fan_in - 1) / merge_fan_in;
+        if (out_len <= kMergeTailThreads) break;  // the rest in one block (msm_merge_tail)
         int src = l & 1, dst = src ^ 1;
         msm_merge<FC><<<grid_for(out_len, 128), 128, 0, s>>>(slot_start.ptr, (uint32_t)active_slots(), seg_len, merge_fan_in, l,
                                                             heads[src].ptr, head_keys[src].ptr, heads[dst].ptr,
                                                             head_keys[dst].ptr, buckets.ptr);
         check_launch("msm_merge");
         len = out_len;
+      }
+      if (l < merge_levels) {
+        msm_merge_tail<FC><<<1, kMergeTailThreads, 0, s>>>(slot_start.ptr, (uint32_t)active_slots(), seg_len,
+                                                         merge_fan_in, l, merge_levels - l, heads[0].ptr,
+                                                         head_keys[0].ptr, heads[1].ptr, head_keys[1].ptr,
+                                                         buckets.ptr);
+        check_launch("msm_merge_tail");
       }
       break;
     }

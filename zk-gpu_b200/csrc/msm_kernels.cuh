@@ -764,20 +764,15 @@ __device__ __forceinline__ void add_into_bucket(uint32_t* buckets, uint32_t key,
   store_xyzz(b, xyzz_add(load_xyzz<F>(b), v));
 }
 
-// Thread u sums heads [u*f, u*f + f) of level `level` (f = fan_in). Runs that start inside the
-// range are added into their bucket; a run that continues from the previous range becomes this
-// thread's head for the next level.
+// Thread u sums heads [u*f, u*f + f) of a level of len heads (f = fan_in). Runs that start
+// inside the range are added into their bucket; a run that continues from the previous range
+// becomes this thread's head for the next level. One add per bucket per level (only the range
+// where a run starts adds it), so a level needs no atomics.
 template <class F>
-__global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ slot_start, uint32_t num_slots,
-                                                 uint32_t seg_len, uint32_t fan_in, uint32_t level,
-                                                 const uint32_t* __restrict__ in_pts,
-                                                 const uint32_t* __restrict__ in_keys, uint32_t* __restrict__ out_pts,
-                                                 uint32_t* __restrict__ out_keys, uint32_t* __restrict__ buckets) {
+__device__ __forceinline__ void merge_range(uint32_t u, uint32_t len, uint32_t fan_in, const uint32_t* __restrict__ in_pts,
+                                            const uint32_t* __restrict__ in_keys, uint32_t* __restrict__ out_pts,
+                                            uint32_t* __restrict__ out_keys, uint32_t* __restrict__ buckets) {
   constexpr int XW = PointWords<F>::xyzz;
-  const uint32_t total = __ldg(&slot_start[num_slots]);
-  const uint32_t len = heads_len(total, seg_len, fan_in, level);
-  if (len <= 1) return;  // nothing left to merge
-  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t q0_64 = (uint64_t)u * fan_in;
   if (q0_64 >= len) return;
   const uint32_t q0 = (uint32_t)q0_64, q1 = min(q0 + fan_in, len);
@@ -804,6 +799,48 @@ __global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ sl
     if (k != kNoKey) acc = xyzz_add(acc, load_xyzz<F>(in_pts + (size_t)q * XW));
   }
   out_keys[u] = out_key;
+}
+
+// One merge level (grid over its output heads).
+template <class F>
+__global__ void __launch_bounds__(128) msm_merge(const uint32_t* __restrict__ slot_start, uint32_t num_slots,
+                                                 uint32_t seg_len, uint32_t fan_in, uint32_t level,
+                                                 const uint32_t* __restrict__ in_pts,
+                                                 const uint32_t* __restrict__ in_keys, uint32_t* __restrict__ out_pts,
+                                                 uint32_t* __restrict__ out_keys, uint32_t* __restrict__ buckets) {
+  const uint32_t total = __ldg(&slot_start[num_slots]);
+  const uint32_t len = heads_len(total, seg_len, fan_in, level);
+  if (len <= 1) return;  // nothing left to merge
+  merge_range<F>(blockIdx.x * blockDim.x + threadIdx.x, len, fan_in, in_pts, in_keys, out_pts, out_keys, buckets);
+}
+
+// The last merge levels, from first_level on, in one block of kMergeTailThreads: every such
+// level has at most kMergeTailThreads output heads (the host starts the tail where the largest
+// possible level fits), the levels run one after another with a block barrier between them
+// (the heads of a level are written by the block before the next reads them), and the
+// ping-pong buffers alternate by level parity as in msm_merge. The small late levels otherwise
+// cost a launch each (about 4-5 us) for a handful of heads.
+constexpr uint32_t kMergeTailThreads = 256;
+template <class F>
+__global__ void __launch_bounds__(kMergeTailThreads) msm_merge_tail(const uint32_t* __restrict__ slot_start,
+                                                                   uint32_t num_slots, uint32_t seg_len, uint32_t fan_in,
+                                                                   uint32_t first_level, uint32_t levels,
+                                                                   uint32_t* __restrict__ heads0,
+                                                                   uint32_t* __restrict__ keys0,
+                                                                   uint32_t* __restrict__ heads1,
+                                                                   uint32_t* __restrict__ keys1,
+                                                                   uint32_t* __restrict__ buckets) {
+  const uint32_t total = __ldg(&slot_start[num_slots]);
+  for (uint32_t l = first_level; l < first_level + levels; l++) {
+    const uint32_t len = heads_len(total, seg_len, fan_in, l);
+    if (len <= 1) break;  // uniform across the block
+    const bool odd = l & 1;
+    const uint32_t out_len = (len + fan_in - 1) / fan_in;
+    for (uint32_t u = threadIdx.x; u < out_len; u += blockDim.x)
+      merge_range<F>(u, len, fan_in, odd ? heads1 : heads0, odd ? keys1 : keys0, odd ? heads0 : heads1,
+                     odd ? keys0 : keys1, buckets);
+    __syncthreads();
+  }
 }
 
 // ------------------------------------------------------------------ bucket reduction
